@@ -1,0 +1,261 @@
+/*
+ * sol_gpu.h — C ABI of the B200 path tracer.
+ *
+ * This is the boundary between SoL's C++ renderer interface and the CUDA
+ * kernels.  Everything crosses it as plain pointers, sizes and PODs; no C++ or
+ * torch types appear.  Each entry point names the SoL interface it stands in
+ * for (paths are relative to the SoL source tree).
+ *
+ * Conventions
+ *  - Every function returns an int status: SOL_GPU_OK (0) or a negative
+ *    SOL_GPU_ERR_* code.  sol_gpu_last_error() returns a message for the last
+ *    failure on the calling thread.
+ *  - Films are planar FP32 RGB, row-major, pixel (0,0) at the top-left, the
+ *    layout of sol::Image's three channels (include/sol/image.h:27-28,97).
+ *    Render calls ADD into the film (sol::Image::accumulate, image.h:54-60) and
+ *    never clear it.
+ *  - A scene handle is bound to the device it was created on; every call sets
+ *    that device first, so handles may be used from any host thread (SoL's
+ *    RenderJob renders on its own std::thread, src/render_job.cpp:25), but one
+ *    handle must not be used by two threads at once.
+ *  - Inputs are copied at creation; the caller keeps ownership of all arrays.
+ */
+#ifndef SOL_GPU_H
+#define SOL_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SOL_GPU_ABI_VERSION 1
+
+/* Status codes */
+#define SOL_GPU_OK                  0
+#define SOL_GPU_ERR_INVALID_ARG    -1
+#define SOL_GPU_ERR_CUDA           -2
+#define SOL_GPU_ERR_OUT_OF_MEMORY  -3
+#define SOL_GPU_ERR_TIMEOUT        -4
+#define SOL_GPU_ERR_QUEUE_OVERFLOW -5
+#define SOL_GPU_ERR_BAD_INDEX      -6
+#define SOL_GPU_ERR_UNSUPPORTED    -7
+#define SOL_GPU_ERR_CANCELLED      -8
+
+/* BSDF kinds, in the order of sol::Bsdf::Tag (include/sol/bsdfs.h:30-36). */
+#define SOL_GPU_BSDF_DIFFUSE 0
+#define SOL_GPU_BSDF_PHONG   1
+#define SOL_GPU_BSDF_MIRROR  2
+#define SOL_GPU_BSDF_GLASS   3
+#define SOL_GPU_BSDF_INTERP  4
+
+/* Texture kinds (include/sol/textures.h:58-64) and image filter / border modes
+ * (textures.h:17-53). */
+#define SOL_GPU_TEX_CONSTANT       0   /* sol::ConstantTexture (scalar) */
+#define SOL_GPU_TEX_CONSTANT_COLOR 1   /* sol::ConstantColorTexture */
+#define SOL_GPU_TEX_IMAGE          2   /* sol::ImageTexture<Filter, Border> */
+#define SOL_GPU_FILTER_NEAREST  0
+#define SOL_GPU_FILTER_BILINEAR 1
+#define SOL_GPU_BORDER_CLAMP  0
+#define SOL_GPU_BORDER_REPEAT 1
+#define SOL_GPU_BORDER_MIRROR 2
+
+/* Light kinds, in the order of sol::Light::Tag (include/sol/lights.h:49-53). */
+#define SOL_GPU_LIGHT_POINT    0
+#define SOL_GPU_LIGHT_TRIANGLE 1   /* sol::UniformTriangleLight */
+#define SOL_GPU_LIGHT_SPHERE   2   /* sol::UniformSphereLight */
+
+/* A texture.  Scalar lookups of colour textures return their luminance
+ * (sol::ColorTexture::sample, textures.h:97-99). */
+typedef struct SolGpuTexture {
+    int32_t type;      /* SOL_GPU_TEX_* */
+    int32_t filter;    /* image: SOL_GPU_FILTER_* */
+    int32_t border;    /* image: SOL_GPU_BORDER_* */
+    int32_t image;     /* image: index into SolGpuSceneDesc.images */
+    float value[3];    /* constant: value[0]; constant colour: r, g, b */
+} SolGpuTexture;
+
+/* An RGB image (sol::Image with three channels). */
+typedef struct SolGpuImage {
+    uint32_t width, height;
+    const float* channels[3];   /* R, G, B planes of width*height floats */
+} SolGpuImage;
+
+/* A BSDF (include/sol/bsdfs.h:97-181). Texture slots by kind:
+ *   diffuse: tex[0] = kd (colour)
+ *   phong:   tex[0] = ks (colour), tex[1] = ns (scalar)
+ *   mirror:  tex[0] = ks (colour)
+ *   glass:   tex[0] = ks (colour), tex[1] = kt (colour), tex[2] = eta (scalar,
+ *            the ratio outside/inside, i.e. 1/IOR as SoL's OBJ loader stores it)
+ *   interp:  tex[0] = k (scalar), a/b = the two BSDFs (neither may be interp) */
+typedef struct SolGpuBsdf {
+    int32_t type;
+    int32_t tex[3];
+    int32_t a, b;
+} SolGpuBsdf;
+
+/* A light (include/sol/lights.h:91-138).
+ *   point:    v0 = position, intensity = colour
+ *   triangle: v0, v1, v2 = the emitting triangle (one-sided: it emits towards
+ *             (v1 - v0) x (v2 - v0)), intensity_tex = colour texture
+ *   sphere:   v0 = centre, v1[0] = radius, intensity_tex = colour texture */
+typedef struct SolGpuLight {
+    int32_t type;
+    int32_t intensity_tex;
+    float intensity[3];
+    float v0[3], v1[3], v2[3];
+} SolGpuLight;
+
+/* One node of a prebuilt binary BVH, as SoL's TriangleMesh holds it after its
+ * own build (src/triangle_mesh.cpp:119-146): node 0 is the root, an inner node
+ * (count == 0) has its children at `first` and `first + 1`, a leaf covers
+ * prim_indices[first .. first + count).  Leaves may hold at most 8 primitives. */
+typedef struct SolGpuBvhNode {
+    float lo[3], hi[3];
+    uint32_t first;
+    uint32_t count;
+} SolGpuBvhNode;
+
+/* Flat scene: the contents of one sol::Scene whose root is a TriangleMesh
+ * (include/sol/scene.h:34-57, include/sol/triangle_mesh.h:18-24). */
+typedef struct SolGpuSceneDesc {
+    uint32_t num_vertices;
+    uint32_t num_triangles;
+    const float* vertices;       /* 3 * num_vertices */
+    const float* normals;        /* 3 * num_vertices, shading normals */
+    const float* tex_coords;     /* 2 * num_vertices */
+    const uint32_t* indices;     /* 3 * num_triangles */
+    const int32_t* tri_bsdf;     /* num_triangles; -1 = no BSDF (path ends there) */
+    const int32_t* tri_light;    /* num_triangles; -1 = not emissive */
+    uint32_t num_bsdfs;    const SolGpuBsdf* bsdfs;
+    uint32_t num_textures; const SolGpuTexture* textures;
+    uint32_t num_images;   const SolGpuImage* images;
+    uint32_t num_lights;   const SolGpuLight* lights;   /* order = sol::Scene::lights */
+    /* Optional prebuilt BVH; when num_bvh_nodes == 0 the library builds one
+     * (full-sweep SAH + reinsertion, as src/triangle_mesh.cpp:142-144 does). */
+    uint32_t num_bvh_nodes;
+    const SolGpuBvhNode* bvh_nodes;
+    const uint32_t* bvh_prim_indices;  /* num_triangles entries */
+} SolGpuSceneDesc;
+
+/* sol::PerspectiveCamera constructor arguments (src/cameras.cpp:5-21). */
+typedef struct SolGpuCamera {
+    float eye[3], dir[3], up[3];
+    float fov;      /* horizontal field of view, degrees */
+    float aspect;   /* width / height */
+} SolGpuCamera;
+
+/* sol::PathTracer::Config (include/sol/algorithms/path_tracer.h:23-29). */
+typedef struct SolGpuConfig {
+    uint32_t max_path_len;
+    uint32_t min_rr_path_len;
+    float min_survival_prob;
+    float max_survival_prob;
+    float ray_offset;
+} SolGpuConfig;
+
+/* Counters of the last render on a scene handle. */
+typedef struct SolGpuRenderStats {
+    uint64_t paths;          /* camera paths traced */
+    uint64_t rays;           /* closest-hit + any-hit rays */
+    uint64_t shadow_rays;    /* any-hit rays */
+    uint64_t nodes_visited;  /* BVH nodes fetched (instrumented renders only) */
+    uint64_t tris_tested;    /* triangles tested (instrumented renders only) */
+    float kernel_ms;         /* device time of the render kernel(s) */
+} SolGpuRenderStats;
+
+/* Description of an uploaded scene. */
+typedef struct SolGpuSceneInfo {
+    uint32_t num_triangles;
+    uint32_t num_nodes;       /* inner nodes of the device BVH */
+    uint32_t bvh_depth;
+    float sah_cost;
+    uint64_t device_bytes;    /* node + triangle + shading arrays */
+    float build_ms;           /* host BVH build + flatten */
+} SolGpuSceneInfo;
+
+/* A ray for sol_gpu_trace: origin, tmin, direction, tmax (8 floats). */
+typedef struct SolGpuRay {
+    float org[3]; float tmin;
+    float dir[3]; float tmax;
+} SolGpuRay;
+
+/* Result of sol_gpu_trace: triangle index in the caller's numbering (-1 = miss),
+ * distance and barycentrics (u weights vertex 1, v weights vertex 2). For any-hit
+ * queries only `tri` is meaningful (>= 0: occluded). */
+typedef struct SolGpuHit {
+    int32_t tri;
+    float t, u, v;
+} SolGpuHit;
+
+typedef struct SolGpuScene SolGpuScene;
+
+/* Message for the last failing call on this thread ("" if none). */
+const char* sol_gpu_last_error(void);
+
+/* ABI version (SOL_GPU_ABI_VERSION). */
+int sol_gpu_abi_version(void);
+
+/* Number of CUDA devices visible to the library. */
+int sol_gpu_device_count(int* count);
+
+/* Builds (or takes) the BVH of a mesh scene and uploads it to `device`.
+ * Replaces the device side of TriangleMesh::TriangleMesh + Scene ownership
+ * (src/triangle_mesh.cpp:44-60, include/sol/scene.h:34-48). */
+int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** out);
+
+/* Frees a scene and its device memory. */
+int sol_gpu_scene_destroy(SolGpuScene* scene);
+
+/* Sizes and build statistics of an uploaded scene. */
+int sol_gpu_scene_info(const SolGpuScene* scene, SolGpuSceneInfo* out);
+
+/* Renders samples [sample_index, sample_index + sample_count) of every pixel
+ * and adds each pixel's sum into the host film channels, exactly as
+ * sol::PathTracer::render does (src/algorithms/path_tracer.cpp:9-23 through
+ * include/sol/renderer.h:34).  Blocking; host<->device copies included. */
+int sol_gpu_render(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config,
+                   uint64_t sample_index, uint32_t sample_count,
+                   uint32_t width, uint32_t height,
+                   float* film_r, float* film_g, float* film_b);
+
+/* Same as sol_gpu_render, but the film is a device buffer of 3*width*height
+ * floats (R plane, G plane, B plane) and the call is asynchronous on `stream`
+ * (a cudaStream_t; NULL = legacy default stream). */
+int sol_gpu_render_device(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config,
+                          uint64_t sample_index, uint32_t sample_count,
+                          uint32_t width, uint32_t height,
+                          float* film_device, void* stream);
+
+/* Counters of the last render on this handle (waits for it to finish). When
+ * `instrumented` was set by sol_gpu_scene_set_instrumented, node and triangle
+ * counts are filled in as well. */
+int sol_gpu_render_stats(SolGpuScene* scene, SolGpuRenderStats* out);
+
+/* Selects the counting variant of the render kernels (slower; for measuring
+ * bytes per ray). */
+int sol_gpu_scene_set_instrumented(SolGpuScene* scene, int instrumented);
+
+/* Closest-hit (any_hit == 0) or any-hit (any_hit != 0) queries for a batch of
+ * device-resident rays, the device side of TriangleMesh::intersect_closest /
+ * intersect_any (src/triangle_mesh.cpp:64-117).  Asynchronous on `stream`. */
+int sol_gpu_trace(SolGpuScene* scene, const SolGpuRay* rays_device, uint32_t count, int any_hit,
+                  SolGpuHit* hits_device, void* stream);
+
+/* Host-only: builds the BVH that TriangleMesh builds for an indexed mesh
+ * (src/triangle_mesh.cpp:119-146: triangle boxes and centroids, full-sweep SAH,
+ * reinsertion), in the SolGpuBvhNode form that SolGpuSceneDesc accepts.
+ * `*num_nodes` holds the capacity of `nodes_out` on entry and the node count on
+ * return; with `nodes_out` or `prim_indices_out` NULL only the count is returned
+ * (at most 2 * num_triangles - 1).  `prim_indices_out` receives num_triangles
+ * entries. */
+int sol_gpu_build_bvh(const float* vertices, uint32_t num_vertices, const uint32_t* indices,
+                      uint32_t num_triangles, SolGpuBvhNode* nodes_out, uint32_t* num_nodes,
+                      uint32_t* prim_indices_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SOL_GPU_H */

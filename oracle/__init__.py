@@ -1,0 +1,170 @@
+"""Test infrastructure: CPU checkers for the GPU path tracer.  Not part of the product.
+
+Two checkers, both over the flat scene of include/sol_gpu.h:
+  * liboracle.so (oracle/_build/): pt_oracle.cpp, a C++ restatement of SoL's
+    path tracer (src/algorithms/path_tracer.cpp and the classes it calls);
+  * libsol_ref.so (oracle/_ref/): SoL's own sources compiled against the
+    clean-room proto/par/bvh shims (oracle/Makefile), driven by ref_harness.cpp.
+
+Only tests, the smoke check and bench.py's CPU-baseline leg use this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "_build" / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libsol_ref.so"
+REF_SOURCES = Path("/root/reference")
+
+_oracle = None
+_ref = None
+
+
+def build(ref: bool = True) -> None:
+    """Builds liboracle.so, and libsol_ref.so when SoL's sources are present."""
+    targets = ["oracle"]
+    if ref and (REF_SOURCES / "src" / "algorithms" / "path_tracer.cpp").exists():
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", str(HERE)] + targets, check=True)
+
+
+def _bind_common():
+    from sol_b200 import capi
+    return capi
+
+
+def oracle_lib() -> C.CDLL:
+    global _oracle
+    if _oracle is None:
+        if not ORACLE_LIB.exists():
+            build(ref=False)
+        capi = _bind_common()
+        lib = C.CDLL(str(ORACLE_LIB))
+        f32p = C.POINTER(C.c_float)
+        lib.oracle_render.argtypes = [C.POINTER(capi.SolGpuSceneDesc), C.POINTER(capi.SolGpuCamera),
+                                      C.POINTER(capi.SolGpuConfig), C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
+                                      f32p, f32p, f32p, C.c_int]
+        lib.oracle_render.restype = C.c_int
+        lib.oracle_trace.argtypes = [C.POINTER(capi.SolGpuSceneDesc), C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]
+        lib.oracle_trace.restype = C.c_int
+        lib.oracle_pcg_floats.argtypes = [C.c_uint64, C.c_uint32, f32p]
+        lib.oracle_pcg_floats.restype = None
+        lib.oracle_pixel_seeds.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        lib.oracle_pixel_seeds.restype = None
+        _oracle = lib
+    return _oracle
+
+
+def ref_available() -> bool:
+    return REF_LIB.exists()
+
+
+def ref_lib() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        if not REF_LIB.exists():
+            raise FileNotFoundError(f"{REF_LIB} is not built (needs SoL's sources; see oracle/Makefile)")
+        capi = _bind_common()
+        lib = C.CDLL(str(REF_LIB))
+        f32p = C.POINTER(C.c_float)
+        lib.ref_scene_create.argtypes = [C.POINTER(capi.SolGpuSceneDesc), C.POINTER(capi.SolGpuCamera)]
+        lib.ref_scene_create.restype = C.c_void_p
+        lib.ref_scene_destroy.argtypes = [C.c_void_p]
+        lib.ref_scene_destroy.restype = None
+        lib.ref_scene_render.argtypes = [C.c_void_p, C.POINTER(capi.SolGpuConfig), C.c_uint64, C.c_uint32,
+                                         C.c_uint32, C.c_uint32, f32p, f32p, f32p, C.c_int, C.POINTER(C.c_double)]
+        lib.ref_scene_render.restype = C.c_int
+        lib.ref_scene_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]
+        lib.ref_scene_trace.restype = C.c_int
+        lib.ref_last_error.argtypes = []
+        lib.ref_last_error.restype = C.c_char_p
+        _ref = lib
+    return _ref
+
+
+def _film(w: int, h: int, film=None) -> np.ndarray:
+    return np.zeros((3, h, w), np.float32) if film is None else np.ascontiguousarray(film, np.float32)
+
+
+def _ptrs(film: np.ndarray):
+    f32p = C.POINTER(C.c_float)
+    return [film[c].ctypes.data_as(f32p) for c in range(3)]
+
+
+def render(scene, config, width: int, height: int, spp: int, sample_index: int = 0, threads: int = 0,
+           camera=None, film=None) -> np.ndarray:
+    """Oracle render: returns the (3, h, w) film after adding `spp` samples per pixel."""
+    desc = scene.desc()
+    cam = (camera or scene.camera).to_c()
+    cfg = config.to_c()
+    out = _film(width, height, film)
+    oracle_lib().oracle_render(desc.ptr, C.byref(cam), C.byref(cfg), sample_index, spp, width, height,
+                               *_ptrs(out), threads)
+    return out
+
+
+def trace(scene, rays: np.ndarray, any_hit: bool) -> np.ndarray:
+    """rays: (n, 8) float32 [org, tmin, dir, tmax] -> hits (n, 4) records (tri:int32, t, u, v)."""
+    desc = scene.desc()
+    rays = np.ascontiguousarray(rays, np.float32)
+    hits = np.zeros((rays.shape[0], 4), np.float32)
+    oracle_lib().oracle_trace(desc.ptr, rays.ctypes.data, rays.shape[0], int(any_hit), hits.ctypes.data)
+    return hits
+
+
+def pcg_floats(seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.float32)
+    oracle_lib().oracle_pcg_floats(seed, n, out.ctypes.data_as(C.POINTER(C.c_float)))
+    return out
+
+
+def pixel_seeds(fxy: np.ndarray) -> np.ndarray:
+    fxy = np.ascontiguousarray(fxy, np.uint64)
+    out = np.zeros(fxy.shape[0], np.uint32)
+    oracle_lib().oracle_pixel_seeds(fxy.ctypes.data, fxy.shape[0], out.ctypes.data)
+    return out
+
+
+class RefScene:
+    """A sol::Scene built by SoL's own constructors, rendered by sol::PathTracer."""
+
+    def __init__(self, scene, camera=None):
+        self._desc = scene.desc()
+        cam = (camera or scene.camera).to_c()
+        self.lib = ref_lib()
+        self.h = self.lib.ref_scene_create(self._desc.ptr, C.byref(cam))
+        if not self.h:
+            raise RuntimeError("ref_scene_create failed: " + self.lib.ref_last_error().decode())
+
+    def render(self, config, width, height, spp, sample_index=0, threads=0, film=None):
+        """Returns (film, render_ms)."""
+        out = _film(width, height, film)
+        ms = C.c_double(0.0)
+        cfg = config.to_c()
+        rc = self.lib.ref_scene_render(self.h, C.byref(cfg), sample_index, spp, width, height, *_ptrs(out),
+                                       threads, C.byref(ms))
+        if rc != 0:
+            raise RuntimeError("ref_scene_render failed: " + self.lib.ref_last_error().decode())
+        return out, ms.value
+
+    def trace(self, rays: np.ndarray, any_hit: bool) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, np.float32)
+        hits = np.zeros((rays.shape[0], 4), np.float32)
+        self.lib.ref_scene_trace(self.h, rays.ctypes.data, rays.shape[0], int(any_hit), hits.ctypes.data)
+        return hits
+
+    def close(self):
+        if self.h:
+            self.lib.ref_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,328 @@
+// C ABI of the B200 path tracer (include/sol_gpu.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/sol_gpu.h"
+#include "core/layout.h"
+#include "host/flatten.h"
+#include "kernels/kernels.h"
+
+using namespace sol_b200;
+
+struct SolGpuScene {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    DNode* nodes = nullptr;
+    DTri* tris = nullptr;
+    DTriShade* shade = nullptr;
+    DBsdf* bsdfs = nullptr;
+    DTexture* textures = nullptr;
+    DImage* images = nullptr;
+    float* texels = nullptr;
+    DLight* lights = nullptr;
+    DeviceCounters* counters = nullptr;
+    float* film_tmp = nullptr;       // device film for host-film renders
+    size_t film_tmp_floats = 0;
+    float* film_host = nullptr;      // pinned staging for host-film renders
+    size_t film_host_floats = 0;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    bool instrumented = false;
+    bool rendered = false;
+    SceneView view{};
+    SolGpuSceneInfo info{};
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    int code = e == cudaErrorMemoryAllocation ? SOL_GPU_ERR_OUT_OF_MEMORY : SOL_GPU_ERR_CUDA;
+    return fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+/// Makes `device` current for the scope of a call and restores the caller's device.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != device) err = cudaSetDevice(device);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+template <typename T>
+cudaError_t upload(T** dst, const std::vector<T>& src) {
+    size_t bytes = std::max<size_t>(sizeof(T), src.size() * sizeof(T));
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(dst), bytes);
+    if (e != cudaSuccess) return e;
+    if (!src.empty()) e = cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+}
+
+void release(SolGpuScene* s) {
+    if (!s) return;
+    DeviceGuard g(s->device);
+    cudaFree(s->nodes); cudaFree(s->tris); cudaFree(s->shade); cudaFree(s->bsdfs);
+    cudaFree(s->textures); cudaFree(s->images); cudaFree(s->texels); cudaFree(s->lights);
+    cudaFree(s->counters); cudaFree(s->film_tmp);
+    if (s->film_host) cudaFreeHost(s->film_host);
+    if (s->ev_start) cudaEventDestroy(s->ev_start);
+    if (s->ev_stop) cudaEventDestroy(s->ev_stop);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+DConfig to_config(const SolGpuConfig& c) {
+    DConfig d;
+    d.max_path_len = c.max_path_len;
+    d.min_rr_path_len = c.min_rr_path_len;
+    d.min_survival_prob = c.min_survival_prob;
+    d.max_survival_prob = c.max_survival_prob;
+    d.ray_offset = c.ray_offset;
+    return d;
+}
+
+int check_render_args(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config,
+                      uint32_t width, uint32_t height) {
+    if (!scene || !camera || !config) return fail(SOL_GPU_ERR_INVALID_ARG, "scene, camera and config must not be NULL");
+    if (width == 0 || height == 0) return fail(SOL_GPU_ERR_INVALID_ARG, "image size must be positive");
+    if ((uint64_t)((width + 7) / 8) * ((height + 3) / 4) * 32 > 0xffffffffull)
+        return fail(SOL_GPU_ERR_INVALID_ARG, "image too large");
+    return SOL_GPU_OK;
+}
+
+int render_into(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config,
+                uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
+                float* film, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(scene->counters, 0, sizeof(DeviceCounters), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    SceneView v = scene->view;
+    int per_sm = megakernel_blocks_per_sm(scene->instrumented);
+    if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
+    int grid = per_sm * scene->num_sms;
+    const DCamera cam = make_camera(*camera);
+    cudaEventRecord(scene->ev_start, stream);
+    e = launch_megakernel(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
+                          scene->counters, scene->instrumented, grid, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "megakernel launch");
+    cudaEventRecord(scene->ev_stop, stream);
+    scene->rendered = true;
+    return SOL_GPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sol_gpu_last_error(void) { return g_last_error.c_str(); }
+
+int sol_gpu_abi_version(void) { return SOL_GPU_ABI_VERSION; }
+
+int sol_gpu_device_count(int* count) {
+    if (!count) return fail(SOL_GPU_ERR_INVALID_ARG, "count must not be NULL");
+    cudaError_t e = cudaGetDeviceCount(count);
+    if (e != cudaSuccess) { *count = 0; return cuda_fail(e, "cudaGetDeviceCount"); }
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** out) {
+    if (!desc || !out) return fail(SOL_GPU_ERR_INVALID_ARG, "desc and out must not be NULL");
+    *out = nullptr;
+    FlatScene flat;
+    std::string err;
+    if (!flatten_scene(*desc, flat, err)) return fail(SOL_GPU_ERR_INVALID_ARG, err);
+
+    DeviceGuard guard(device);
+    if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
+    auto* s = new SolGpuScene();
+    s->device = device;
+    cudaError_t e = cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_start);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev_stop);
+    if (e == cudaSuccess) e = upload(&s->nodes, flat.nodes);
+    if (e == cudaSuccess) e = upload(&s->tris, flat.tris);
+    if (e == cudaSuccess) e = upload(&s->shade, flat.shade);
+    if (e == cudaSuccess) e = upload(&s->bsdfs, flat.bsdfs);
+    if (e == cudaSuccess) e = upload(&s->textures, flat.textures);
+    if (e == cudaSuccess) e = upload(&s->images, flat.images);
+    if (e == cudaSuccess) e = upload(&s->texels, flat.texels);
+    if (e == cudaSuccess) e = upload(&s->lights, flat.lights);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s->counters), sizeof(DeviceCounters));
+    if (e != cudaSuccess) { int rc = cuda_fail(e, "scene upload"); release(s); return rc; }
+
+    s->view.nodes = s->nodes;
+    s->view.tris = s->tris;
+    s->view.shade = s->shade;
+    s->view.bsdfs = s->bsdfs;
+    s->view.textures = s->textures;
+    s->view.images = s->images;
+    s->view.texels = s->texels;
+    s->view.lights = s->lights;
+    s->view.num_lights = (uint32_t)flat.lights.size();
+    s->view.num_tris = desc->num_triangles;
+
+    s->info.num_triangles = desc->num_triangles;
+    s->info.num_nodes = (uint32_t)flat.nodes.size();
+    s->info.bvh_depth = flat.depth;
+    s->info.sah_cost = flat.sah_cost;
+    s->info.device_bytes = flat.nodes.size() * sizeof(DNode) + flat.tris.size() * sizeof(DTri) +
+                           flat.shade.size() * sizeof(DTriShade);
+    s->info.build_ms = (float)flat.build_ms;
+    *out = s;
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_scene_destroy(SolGpuScene* scene) {
+    if (!scene) return fail(SOL_GPU_ERR_INVALID_ARG, "scene must not be NULL");
+    {
+        DeviceGuard g(scene->device);
+        if (scene->stream) cudaStreamSynchronize(scene->stream);
+    }
+    release(scene);
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_scene_info(const SolGpuScene* scene, SolGpuSceneInfo* out) {
+    if (!scene || !out) return fail(SOL_GPU_ERR_INVALID_ARG, "scene and out must not be NULL");
+    *out = scene->info;
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_scene_set_instrumented(SolGpuScene* scene, int instrumented) {
+    if (!scene) return fail(SOL_GPU_ERR_INVALID_ARG, "scene must not be NULL");
+    scene->instrumented = instrumented != 0;
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_render_device(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config,
+                          uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
+                          float* film_device, void* stream) {
+    int rc = check_render_args(scene, camera, config, width, height);
+    if (rc != SOL_GPU_OK) return rc;
+    if (!film_device) return fail(SOL_GPU_ERR_INVALID_ARG, "film must not be NULL");
+    DeviceGuard guard(scene->device);
+    if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
+    return render_into(scene, camera, config, sample_index, sample_count, width, height, film_device,
+                       static_cast<cudaStream_t>(stream));
+}
+
+int sol_gpu_render(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config,
+                   uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
+                   float* film_r, float* film_g, float* film_b) {
+    int rc = check_render_args(scene, camera, config, width, height);
+    if (rc != SOL_GPU_OK) return rc;
+    if (!film_r || !film_g || !film_b) return fail(SOL_GPU_ERR_INVALID_ARG, "film channels must not be NULL");
+    DeviceGuard guard(scene->device);
+    if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
+    const size_t plane = (size_t)width * height;
+    const size_t floats = 3 * plane;
+    cudaError_t e = cudaSuccess;
+    if (scene->film_tmp_floats < floats) {
+        cudaFree(scene->film_tmp);
+        scene->film_tmp = nullptr;
+        scene->film_tmp_floats = 0;
+        e = cudaMalloc(reinterpret_cast<void**>(&scene->film_tmp), floats * sizeof(float));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc film");
+        scene->film_tmp_floats = floats;
+    }
+    if (scene->film_host_floats < floats) {
+        if (scene->film_host) cudaFreeHost(scene->film_host);
+        scene->film_host = nullptr;
+        scene->film_host_floats = 0;
+        e = cudaMallocHost(reinterpret_cast<void**>(&scene->film_host), floats * sizeof(float));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMallocHost film");
+        scene->film_host_floats = floats;
+    }
+    e = cudaMemsetAsync(scene->film_tmp, 0, floats * sizeof(float), scene->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync film");
+    rc = render_into(scene, camera, config, sample_index, sample_count, width, height, scene->film_tmp, scene->stream);
+    if (rc != SOL_GPU_OK) return rc;
+    e = cudaMemcpyAsync(scene->film_host, scene->film_tmp, floats * sizeof(float), cudaMemcpyDeviceToHost, scene->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(scene->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "render");
+    // Image::accumulate: one add per pixel and channel (include/sol/image.h:54-60).
+    const float* src = scene->film_host;
+    float* dst[3] = {film_r, film_g, film_b};
+    #pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)plane; ++i)
+        for (int c = 0; c < 3; ++c) dst[c][i] += src[c * plane + i];
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_render_stats(SolGpuScene* scene, SolGpuRenderStats* out) {
+    if (!scene || !out) return fail(SOL_GPU_ERR_INVALID_ARG, "scene and out must not be NULL");
+    std::memset(out, 0, sizeof(*out));
+    if (!scene->rendered) return SOL_GPU_OK;
+    DeviceGuard guard(scene->device);
+    cudaError_t e = cudaEventSynchronize(scene->ev_stop);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventSynchronize");
+    DeviceCounters c;
+    e = cudaMemcpy(&c, scene->counters, sizeof(c), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy counters");
+    out->paths = c.paths;
+    out->rays = c.rays;
+    out->shadow_rays = c.shadow_rays;
+    out->nodes_visited = c.nodes;
+    out->tris_tested = c.tris;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, scene->ev_start, scene->ev_stop) == cudaSuccess) out->kernel_ms = ms;
+    if (c.error) return fail(SOL_GPU_ERR_BAD_INDEX, "device reported an error");
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_trace(SolGpuScene* scene, const SolGpuRay* rays_device, uint32_t count, int any_hit,
+                  SolGpuHit* hits_device, void* stream) {
+    if (!scene || (count > 0 && (!rays_device || !hits_device)))
+        return fail(SOL_GPU_ERR_INVALID_ARG, "scene, rays and hits must not be NULL");
+    DeviceGuard guard(scene->device);
+    if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
+    if (scene->view.num_tris == 0) {
+        // No geometry: every query misses.
+        cudaError_t e = cudaMemsetAsync(hits_device, 0xff, sizeof(SolGpuHit) * count, static_cast<cudaStream_t>(stream));
+        return e == cudaSuccess ? SOL_GPU_OK : cuda_fail(e, "cudaMemsetAsync");
+    }
+    cudaError_t e = launch_trace(scene->view, rays_device, count, any_hit != 0, hits_device,
+                                 static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? SOL_GPU_OK : cuda_fail(e, "trace launch");
+}
+
+int sol_gpu_build_bvh(const float* vertices, uint32_t num_vertices, const uint32_t* indices, uint32_t num_triangles,
+                      SolGpuBvhNode* nodes_out, uint32_t* num_nodes, uint32_t* prim_indices_out) {
+    if (!num_nodes) return fail(SOL_GPU_ERR_INVALID_ARG, "num_nodes must not be NULL");
+    if (num_triangles > 0 && (!vertices || !indices)) return fail(SOL_GPU_ERR_INVALID_ARG, "mesh arrays must not be NULL");
+    for (size_t i = 0; i < 3 * (size_t)num_triangles; ++i)
+        if (indices[i] >= num_vertices) return fail(SOL_GPU_ERR_INVALID_ARG, "vertex index out of range");
+    if (num_triangles == 0) { *num_nodes = 0; return SOL_GPU_OK; }
+    bvh::Bvh tree = build_mesh_bvh(vertices, indices, num_triangles);
+    const uint32_t capacity = *num_nodes;
+    *num_nodes = (uint32_t)tree.nodes.size();
+    if (!nodes_out || !prim_indices_out) return SOL_GPU_OK;   // size query
+    if (capacity < tree.nodes.size()) return fail(SOL_GPU_ERR_INVALID_ARG, "node buffer too small");
+    for (size_t i = 0; i < tree.nodes.size(); ++i) {
+        const bvh::Node& n = tree.nodes[i];
+        for (int k = 0; k < 3; ++k) { nodes_out[i].lo[k] = n.box.lo[k]; nodes_out[i].hi[k] = n.box.hi[k]; }
+        nodes_out[i].first = n.first;
+        nodes_out[i].count = n.count;
+    }
+    std::memcpy(prim_indices_out, tree.prim_indices.data(), sizeof(uint32_t) * num_triangles);
+    return SOL_GPU_OK;
+}
+
+}  // extern "C"

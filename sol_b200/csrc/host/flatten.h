@@ -1,0 +1,38 @@
+// Scene validation and flattening into the device layout (host only).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../core/layout.h"
+#include "../../../include/sol_gpu.h"
+#include "bvh_builder.h"
+
+namespace sol_b200 {
+
+struct FlatScene {
+    std::vector<DNode> nodes;
+    std::vector<DTri> tris;
+    std::vector<DTriShade> shade;
+    std::vector<DBsdf> bsdfs;
+    std::vector<DTexture> textures;
+    std::vector<DImage> images;
+    std::vector<float> texels;
+    std::vector<DLight> lights;
+    uint32_t depth = 0;
+    float sah_cost = 0.0f;
+    double build_ms = 0.0;
+};
+
+/// Builds the BVH SoL's TriangleMesh builds for a mesh (src/triangle_mesh.cpp:119-146):
+/// triangle boxes and centroids, full-sweep SAH, then reinsertion.
+bvh::Bvh build_mesh_bvh(const float* vertices, const uint32_t* indices, size_t num_triangles);
+
+/// Validates `desc` and produces the device layout. Returns false with a message
+/// in `err` on invalid input.
+bool flatten_scene(const SolGpuSceneDesc& desc, FlatScene& out, std::string& err);
+
+/// PerspectiveCamera's constructor (src/cameras.cpp:5-21).
+DCamera make_camera(const SolGpuCamera& c);
+
+}  // namespace sol_b200

@@ -1,0 +1,30 @@
+// Host-side launchers of the CUDA kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../core/layout.h"
+#include "../../../include/sol_gpu.h"
+
+namespace sol_b200 {
+
+constexpr int kMegakernelBlock = 128;
+constexpr int kTraceBlock = 128;
+
+/// Resident blocks per SM of the megakernel (for sizing its persistent grid).
+int megakernel_blocks_per_sm(bool instrumented);
+
+/// K1: renders samples [sample_index, sample_index + sample_count) of every
+/// pixel and adds each pixel's sum into `film` (3 planes of width*height).
+/// `counters` must be zeroed before the launch.
+cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DConfig& cfg,
+                              uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
+                              float* film, DeviceCounters* counters, bool instrumented, int grid,
+                              cudaStream_t stream);
+
+/// K9: closest-hit or any-hit queries for a batch of rays.
+cudaError_t launch_trace(const SceneView& s, const SolGpuRay* rays, uint32_t count, bool any_hit,
+                         SolGpuHit* hits, cudaStream_t stream);
+
+}  // namespace sol_b200

@@ -1,0 +1,101 @@
+// BVH2 traversal on the device: the GPU statement of
+// TriangleMesh::intersect_closest / intersect_any (src/triangle_mesh.cpp:64-117),
+// which SoL runs through bvh v2's SingleRayTraverser.
+//
+// Layout: every inner node is 64 bytes holding both child boxes, fetched as four
+// 128-bit read-only loads; triangles are 48 bytes (three 128-bit loads).  The
+// traversal is the stack-based "while-while" loop of Aila & Laine ("Understanding
+// the Efficiency of Ray Traversal on GPUs", HPG 2009): descend inner nodes
+// nearest-child first, pushing the farther child, until a leaf is reached; then
+// test the leaf's triangles.  Box tests use one FMA per slab and widen the exit
+// distance by kSlabWiden so that they are conservative; the triangle test is
+// the shared watertight test, so a hit found here is bit-identical to the one the
+// host checker finds.
+#pragma once
+
+#include "../core/layout.h"
+#include "../core/math.h"
+
+namespace sol_b200 {
+
+struct TraversalCounters {
+    uint32_t nodes;
+    uint32_t tris;
+};
+
+__device__ __forceinline__ float4 ldg4(const void* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+__device__ __forceinline__ Vec3 tri_vertex(float4 a) { return vec3(a.x, a.y, a.z); }
+
+/// Traverses the BVH for one ray.  For kAnyHit the first triangle hit inside
+/// (tmin, tmax) is returned; otherwise the closest one, with `tmax` shrunk to
+/// its distance.  Returns the triangle's position in leaf order, or -1.
+/// `active == false` lanes return -1 at once but keep the warp convergent.
+template <bool kAnyHit, bool kCount>
+__device__ __forceinline__ int traverse(const DNode* __restrict__ nodes, const DTri* __restrict__ tris,
+                                        Vec3 org, Vec3 dir, float tmin, float& tmax, bool active,
+                                        TraversalCounters& ctr) {
+    int stack[kTraversalStack];
+    int sp = 0;
+    int hit = -1;
+    const Vec3 idir = safe_inverse(dir);
+    const Vec3 ood = vec3(-org.x * idir.x, -org.y * idir.y, -org.z * idir.z);
+    const RayShear rs = make_shear(org, dir);
+    int node = active ? 0 : kStackSentinel;
+    stack[sp++] = kStackSentinel;
+
+    while (node != kStackSentinel) {
+        // Descend inner nodes until a leaf (or the end) is reached.
+        while (node >= 0) {
+            const DNode* n = nodes + node;
+            const float4 a = ldg4(n->b0);
+            const float4 b = ldg4(n->b1);
+            const float4 c = ldg4(n->b2);
+            const int4 r = __ldg(reinterpret_cast<const int4*>(n->ref));
+            if (kCount) ctr.nodes++;
+            float t0lx = __fmaf_rn(a.x, idir.x, ood.x), t0hx = __fmaf_rn(a.y, idir.x, ood.x);
+            float t0ly = __fmaf_rn(a.z, idir.y, ood.y), t0hy = __fmaf_rn(a.w, idir.y, ood.y);
+            float t0lz = __fmaf_rn(c.x, idir.z, ood.z), t0hz = __fmaf_rn(c.y, idir.z, ood.z);
+            float t1lx = __fmaf_rn(b.x, idir.x, ood.x), t1hx = __fmaf_rn(b.y, idir.x, ood.x);
+            float t1ly = __fmaf_rn(b.z, idir.y, ood.y), t1hy = __fmaf_rn(b.w, idir.y, ood.y);
+            float t1lz = __fmaf_rn(c.z, idir.z, ood.z), t1hz = __fmaf_rn(c.w, idir.z, ood.z);
+            float n0 = fmaxf(fmaxf(fminf(t0lx, t0hx), fminf(t0ly, t0hy)), fmaxf(fminf(t0lz, t0hz), tmin));
+            float f0 = fminf(fminf(fmaxf(t0lx, t0hx), fmaxf(t0ly, t0hy)), fminf(fmaxf(t0lz, t0hz), tmax)) * kSlabWiden;
+            float n1 = fmaxf(fmaxf(fminf(t1lx, t1hx), fminf(t1ly, t1hy)), fmaxf(fminf(t1lz, t1hz), tmin));
+            float f1 = fminf(fminf(fmaxf(t1lx, t1hx), fmaxf(t1ly, t1hy)), fminf(fmaxf(t1lz, t1hz), tmax)) * kSlabWiden;
+            const bool h0 = n0 <= f0, h1 = n1 <= f1;
+            if (h0 && h1) {
+                int near = r.x, far = r.y;
+                if (n1 < n0) { near = r.y; far = r.x; }
+                stack[sp++] = far;
+                node = near;
+            } else if (h0) {
+                node = r.x;
+            } else if (h1) {
+                node = r.y;
+            } else {
+                node = stack[--sp];
+            }
+        }
+        if (node == kStackSentinel) break;
+        // Leaf: ~node = (first << 3) | (count - 1)
+        const uint32_t v = ~(uint32_t)node;
+        const uint32_t first = v >> 3, count = (v & 7u) + 1u;
+        for (uint32_t i = first; i < first + count; ++i) {
+            const DTri* tp = tris + i;
+            const float4 p0 = ldg4(tp->v0), p1 = ldg4(tp->v1), p2 = ldg4(tp->v2);
+            if (kCount) ctr.tris++;
+            float t, u, w;
+            if (intersect_triangle(rs, tri_vertex(p0), tri_vertex(p1), tri_vertex(p2), tmin, tmax, &t, &u, &w)) {
+                hit = (int)i;
+                tmax = t;
+                if (kAnyHit) break;
+            }
+        }
+        if (kAnyHit && hit >= 0) break;
+        node = stack[--sp];
+    }
+    return hit;
+}
+
+}  // namespace sol_b200
