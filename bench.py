@@ -1,0 +1,321 @@
+"""Benchmark of the B200 path tracer (one JSON line on rank 0).
+
+Workload: the plain per-pixel megakernel on the sphere field of 1,048,576
+sphere triangles (+ 2 ground, 8 light triangles), 1920x1080, 64 samples per pixel,
+maximum path length 8 -- one step renders that whole frame (132,710,400 paths).
+With N GPUs (torchrun) every rank renders its own 64-sample range of the same
+frame (weak scaling: independent sample ranges, no collective on the data path).
+
+  value  device-timed Mpaths/s of the render kernel (scene resident on the GPU,
+         L2 flushed between steps), summed over ranks
+  e2e    Mpaths/s through the C ABI entry point a SoL renderer calls
+         (sol_gpu_render with the host film: the film's device->host copy and
+         the host-side accumulate are inside the timed region)
+
+`--impl reference` times SoL's own CPU path tracer (oracle/_ref, or the oracle
+restatement when SoL's sources were not built) on all host threads instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = {"workload": "plain megakernel, sphere field (64 displaced UV spheres x 16,384 tris + 10), "
+                        "1920x1080, 64 spp, max path length 8",
+            "triangles": 1048586, "width": 1920, "height": 1080, "spp": 64, "max_path_len": 8,
+            "l2": "flushed between steps (256 MiB write)"}
+METRIC = "Mpaths/s"
+BASELINE_VALUE = None   # no published number exists for this metric
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--small", action="store_true", help="quick run on a reduced frame (not a bench number)")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() in ("active", "1", "yes"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_workload(small: bool):
+    from sol_b200 import scenes
+    scene = scenes.sphere_field(64, seed=1)
+    w, h, spp = (480, 270, 8) if small else (1920, 1080, 64)
+    return scene, scenes.SPHERES_CONFIG, w, h, spp
+
+
+def cpu_reference_mpaths(scene, cfg, w, h, target_s: float = 12.0, max_spp: int = 64):
+    """SoL's own path tracer on all host threads over whole frames; 1 spp first,
+    then enough samples for about `target_s` seconds (paths are independent)."""
+    import oracle
+    threads = os.cpu_count() or 1
+    if oracle.ref_available():
+        ref = oracle.RefScene(scene)
+        kind = "reference"
+
+        def run(index, spp):
+            _, ms = ref.render(cfg, w, h, spp, sample_index=index, threads=threads)
+            return ms / 1000.0
+    else:
+        kind = "port"
+
+        def run(index, spp):
+            t = time.perf_counter()
+            oracle.render(scene, cfg, w, h, spp, sample_index=index, threads=threads)
+            return time.perf_counter() - t
+    t1 = run(0, 1)
+    spp = int(min(max_spp, max(1, math.floor(target_s / max(t1, 1e-3)))))
+    t = run(1, spp) if spp > 1 else t1
+    paths = w * h * spp
+    return {"value": paths / t / 1e6, "unit": METRIC, "cores": threads, "kind": kind,
+            "sample": f"{spp} spp of the full {w}x{h} frame ({paths} paths) on {threads} threads, "
+                      f"{t:.2f} s; BVH build excluded (test/driver.cpp:232 starts the clock after scene load)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    scene, cfg, w, h, _ = make_workload(args.small)
+    import oracle
+    threads = os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available() else "port"
+    ref = oracle.RefScene(scene) if kind == "reference" else None
+
+    def step(index, spp=1):
+        if ref is not None:
+            _, ms = ref.render(cfg, w, h, spp, sample_index=index, threads=threads)
+            return ms / 1000.0
+        t = time.perf_counter()
+        oracle.render(scene, cfg, w, h, spp, sample_index=index, threads=threads)
+        return time.perf_counter() - t
+    for i in range(args.warmup):
+        step(i)
+    times = [step(args.warmup + i) for i in range(args.steps)]
+    total = sum(times)
+    paths = w * h * args.steps
+    value = paths / total / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(WORKLOAD, step="1 spp of the full frame per step (bounded CPU sample)"),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": kind,
+                             "sample": f"1 spp of the full {w}x{h} frame per step, {args.steps} steps"},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from sol_b200 import build
+    build.build()
+    from sol_b200.renderer import GpuPathTracer, GpuScene, Image
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+
+    scene, cfg, w, h, spp = make_workload(args.small)
+    gscene = GpuScene(scene, device=local)
+    info = gscene.info()
+    pt = GpuPathTracer(gscene, cfg)
+    film = torch.zeros((3, h, w), dtype=torch.float32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    base = rank * spp * (args.warmup + args.steps + 1)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def reduce_max(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # Warm-up.
+    for i in range(args.warmup):
+        pt.render_device(film.data_ptr(), w, h, base + i * spp, spp, stream.cuda_stream)
+    barrier()
+
+    # Device-timed steps: L2 flushed before each, render timed with events on its stream.
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        barrier()
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            pt.render_device(film.data_ptr(), w, h, base + (args.warmup + i) * spp, spp, stream.cuda_stream)
+            ev[i][1].record(stream)
+        barrier()
+        wall = time.perf_counter() - t0
+    kernel_s = sum(a.elapsed_time(b) for a, b in ev) / 1000.0
+    kernel_s = reduce_max(kernel_s)
+    st = pt.stats()
+    rays_per_step = st.rays
+
+    # Algorithmic bytes per launch from the counting variant of the same render.
+    gscene.set_instrumented(True)
+    pt.render_device(film.data_ptr(), w, h, base, spp, stream.cuda_stream)
+    torch.cuda.synchronize()
+    ist = pt.stats()
+    gscene.set_instrumented(False)
+    alg_bytes = 64.0 * ist.nodes_visited + 48.0 * ist.tris_tested + 32.0 * ist.rays
+
+    # End to end through the C ABI with the host film.
+    img = Image(w, h)
+    pt.render(img, base, spp)                     # warm the staging buffers
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        pt.render(img, base + i * spp, spp)
+    barrier()
+    e2e_s = reduce_max(time.perf_counter() - t0)
+
+    from sol_b200 import capi
+    import ctypes
+    # Per-step inputs: camera, configuration and the sample range, passed by value to the kernel.
+    h2d_bytes = ctypes.sizeof(capi.SolGpuCamera) + ctypes.sizeof(capi.SolGpuConfig) + 8 + 4 * 3
+    paths = float(w * h * spp)
+    value = world * paths * args.steps / kernel_s / 1e6
+    e2e = world * paths * args.steps / e2e_s / 1e6
+    peak, peak_src = load_peaks()
+    achieved = alg_bytes / (kernel_s / args.steps) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "megakernel_sphere_field_traffic.json"
+    if tfile.exists() and not args.small:
+        traffic = json.loads(tfile.read_text()).get("dram_bytes_per_launch")
+    line = None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * kernel_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None if BASELINE_VALUE is None else value / BASELINE_VALUE,
+            "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": dict(WORKLOAD, parallelism=f"{world} GPU(s), one 64-sample range per rank",
+                           small=bool(args.small)),
+            "mrays_per_s": world * rays_per_step * args.steps / kernel_s / 1e6,
+            "rays_per_path": rays_per_step / paths,
+            "bytes_per_ray": alg_bytes / ist.rays,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d_bytes,
+                    "d2h_bytes_per_step": int(3 * w * h * 4)},
+            "gpu_launches": args.steps,
+            "clocks": clocks.summary(),
+            "wall_s_timed_region": wall,
+            "scene": {"triangles": info.num_triangles, "bvh_inner_nodes": info.num_nodes,
+                      "bvh_depth": info.bvh_depth, "sah_cost": info.sah_cost,
+                      "device_mb": info.device_bytes / 2**20, "build_ms": info.build_ms},
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_reference_mpaths(scene, cfg, w, h)
+            except Exception as e:   # reported, not fatal
+                line["cpu_baseline"] = {"value": None, "error": str(e)}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

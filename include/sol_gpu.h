@@ -139,11 +139,15 @@ typedef struct SolGpuSceneDesc {
     const uint32_t* bvh_prim_indices;  /* num_triangles entries */
 } SolGpuSceneDesc;
 
-/* sol::PerspectiveCamera constructor arguments (src/cameras.cpp:5-21). */
+/* A constructed sol::PerspectiveCamera (include/sol/cameras.h:50-54): the eye,
+ * the unit view direction, and the right / up vectors already scaled by the
+ * half extents of the image plane.  Rays are generated as in
+ * PerspectiveCamera::generate_ray (src/cameras.cpp:23-25). */
 typedef struct SolGpuCamera {
-    float eye[3], dir[3], up[3];
-    float fov;      /* horizontal field of view, degrees */
-    float aspect;   /* width / height */
+    float eye[3];
+    float dir[3];
+    float right[3];
+    float up[3];
 } SolGpuCamera;
 
 /* sol::PathTracer::Config (include/sol/algorithms/path_tracer.h:23-29). */
@@ -205,6 +209,11 @@ int sol_gpu_device_count(int* count);
  * (src/triangle_mesh.cpp:44-60, include/sol/scene.h:34-48). */
 int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** out);
 
+/* sol::PerspectiveCamera's constructor (src/cameras.cpp:5-21): `fov` is the
+ * horizontal field of view in degrees, `aspect` = width / height. */
+int sol_gpu_camera_perspective(const float eye[3], const float dir[3], const float up[3], float fov, float aspect,
+                               SolGpuCamera* out);
+
 /* Frees a scene and its device memory. */
 int sol_gpu_scene_destroy(SolGpuScene* scene);
 
@@ -242,6 +251,59 @@ int sol_gpu_scene_set_instrumented(SolGpuScene* scene, int instrumented);
  * intersect_any (src/triangle_mesh.cpp:64-117).  Asynchronous on `stream`. */
 int sol_gpu_trace(SolGpuScene* scene, const SolGpuRay* rays_device, uint32_t count, int any_hit,
                   SolGpuHit* hits_device, void* stream);
+
+/* ---- Batched rendering: many views over one or more scenes ------------------
+ *
+ * The batch renderer traces all paths of all views of one call through a
+ * persistent wavefront (generate / extend / shade / shadow stages over queues
+ * in device memory, hits binned by BSDF kind) whose bounce loop runs inside one
+ * CUDA graph.  Every view's film receives exactly what sol_gpu_render_device
+ * would add for the same camera and sample range, bit for bit.  There is no
+ * SoL counterpart (SoL renders one image per call); it batches
+ * PathTracer::render (src/algorithms/path_tracer.cpp:9-23). */
+
+/* One view of a batch. */
+typedef struct SolGpuView {
+    uint32_t scene;          /* index into the scenes given to sol_gpu_batch_create */
+    SolGpuCamera camera;
+    uint32_t width, height;
+    uint64_t sample_index;
+    uint32_t sample_count;
+    float* film;             /* device film of 3*width*height floats (R, G, B planes); added into */
+} SolGpuView;
+
+/* Tuning of the batch renderer; zero fields take defaults. */
+typedef struct SolGpuBatchOptions {
+    uint32_t capacity;        /* path slots in flight (default: 1M, at most the pixel count) */
+    uint32_t block_size;      /* threads per block of the stages: 64, 128 or 256 (default 128) */
+    uint32_t sort_threshold;  /* bin hits by BSDF kind when at least this many rays are queued
+                                 (0 = always; 0xffffffff = never) */
+    int32_t host_loop;        /* 1: bounce loop driven from the host instead of the graph */
+} SolGpuBatchOptions;
+
+typedef struct SolGpuBatch SolGpuBatch;
+
+/* Creates a batch renderer over `num_scenes` scenes (all on one device). */
+int sol_gpu_batch_create(SolGpuScene* const* scenes, uint32_t num_scenes, const SolGpuBatchOptions* options,
+                         SolGpuBatch** out);
+
+/* Frees a batch renderer (the scenes stay alive). */
+int sol_gpu_batch_destroy(SolGpuBatch* batch);
+
+/* Renders every view's sample range into its film; asynchronous on `stream`. */
+int sol_gpu_batch_render(SolGpuBatch* batch, const SolGpuConfig* config, const SolGpuView* views,
+                         uint32_t num_views, void* stream);
+
+/* Counters and device time of the last batch render (waits for it). */
+int sol_gpu_batch_stats(SolGpuBatch* batch, SolGpuRenderStats* out);
+
+/* Times candidate options (capacity, block size, binning threshold) on one
+ * sample per pixel of the given views, rendered into scratch films, adopts the
+ * fastest and returns it in `chosen`.  With `cache_path` set, a previous
+ * choice for the same device and batch shape is read from that file instead,
+ * and new choices are appended to it. */
+int sol_gpu_batch_autotune(SolGpuBatch* batch, const SolGpuConfig* config, const SolGpuView* views,
+                           uint32_t num_views, const char* cache_path, SolGpuBatchOptions* chosen);
 
 /* Host-only: builds the BVH that TriangleMesh builds for an indexed mesh
  * (src/triangle_mesh.cpp:119-146: triangle boxes and centroids, full-sweep SAH,

@@ -38,6 +38,22 @@ def _bind_common():
     return capi
 
 
+class CameraArgs(C.Structure):
+    """OracleCamera: sol::PerspectiveCamera constructor arguments."""
+    _fields_ = [("eye", C.c_float * 3), ("dir", C.c_float * 3), ("up", C.c_float * 3),
+                ("fov", C.c_float), ("aspect", C.c_float)]
+
+
+def camera_args(camera) -> CameraArgs:
+    c = CameraArgs()
+    c.eye[:] = camera.eye
+    c.dir[:] = camera.dir
+    c.up[:] = camera.up
+    c.fov = camera.fov
+    c.aspect = camera.aspect
+    return c
+
+
 def oracle_lib() -> C.CDLL:
     global _oracle
     if _oracle is None:
@@ -46,7 +62,7 @@ def oracle_lib() -> C.CDLL:
         capi = _bind_common()
         lib = C.CDLL(str(ORACLE_LIB))
         f32p = C.POINTER(C.c_float)
-        lib.oracle_render.argtypes = [C.POINTER(capi.SolGpuSceneDesc), C.POINTER(capi.SolGpuCamera),
+        lib.oracle_render.argtypes = [C.POINTER(capi.SolGpuSceneDesc), C.POINTER(CameraArgs),
                                       C.POINTER(capi.SolGpuConfig), C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
                                       f32p, f32p, f32p, C.c_int]
         lib.oracle_render.restype = C.c_int
@@ -72,7 +88,7 @@ def ref_lib() -> C.CDLL:
         capi = _bind_common()
         lib = C.CDLL(str(REF_LIB))
         f32p = C.POINTER(C.c_float)
-        lib.ref_scene_create.argtypes = [C.POINTER(capi.SolGpuSceneDesc), C.POINTER(capi.SolGpuCamera)]
+        lib.ref_scene_create.argtypes = [C.POINTER(capi.SolGpuSceneDesc), C.POINTER(CameraArgs)]
         lib.ref_scene_create.restype = C.c_void_p
         lib.ref_scene_destroy.argtypes = [C.c_void_p]
         lib.ref_scene_destroy.restype = None
@@ -81,6 +97,12 @@ def ref_lib() -> C.CDLL:
         lib.ref_scene_render.restype = C.c_int
         lib.ref_scene_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]
         lib.ref_scene_trace.restype = C.c_int
+        lib.ref_adapter_render.argtypes = [C.c_void_p, C.POINTER(capi.SolGpuConfig), C.c_uint64, C.c_uint32,
+                                           C.c_uint32, C.c_uint32, f32p, f32p, f32p, C.c_int, C.c_int, C.c_uint32]
+        lib.ref_adapter_render.restype = C.c_int
+        lib.ref_renderjob_render.argtypes = [C.c_void_p, C.POINTER(capi.SolGpuConfig), C.c_uint32, C.c_uint32,
+                                             C.c_uint32, C.c_uint32, f32p, f32p, f32p, C.c_int]
+        lib.ref_renderjob_render.restype = C.c_int
         lib.ref_last_error.argtypes = []
         lib.ref_last_error.restype = C.c_char_p
         _ref = lib
@@ -100,7 +122,7 @@ def render(scene, config, width: int, height: int, spp: int, sample_index: int =
            camera=None, film=None) -> np.ndarray:
     """Oracle render: returns the (3, h, w) film after adding `spp` samples per pixel."""
     desc = scene.desc()
-    cam = (camera or scene.camera).to_c()
+    cam = camera_args(camera or scene.camera)
     cfg = config.to_c()
     out = _film(width, height, film)
     oracle_lib().oracle_render(desc.ptr, C.byref(cam), C.byref(cfg), sample_index, spp, width, height,
@@ -135,7 +157,7 @@ class RefScene:
 
     def __init__(self, scene, camera=None):
         self._desc = scene.desc()
-        cam = (camera or scene.camera).to_c()
+        cam = camera_args(camera or scene.camera)
         self.lib = ref_lib()
         self.h = self.lib.ref_scene_create(self._desc.ptr, C.byref(cam))
         if not self.h:
@@ -151,6 +173,24 @@ class RefScene:
         if rc != 0:
             raise RuntimeError("ref_scene_render failed: " + self.lib.ref_last_error().decode())
         return out, ms.value
+
+    def render_gpu_dropin(self, config, width, height, spp, sample_index=0, device=0, render_job=False,
+                          samples_per_frame=0, film=None):
+        """The same sol::Scene rendered by sol::GpuPathTracer (the product's drop-in)."""
+        out = _film(width, height, film)
+        cfg = config.to_c()
+        rc = self.lib.ref_adapter_render(self.h, C.byref(cfg), sample_index, spp, width, height, *_ptrs(out),
+                                         device, int(render_job), samples_per_frame or spp)
+        if rc != 0:
+            raise RuntimeError("sol::GpuPathTracer failed: " + self.lib.ref_last_error().decode())
+        return out
+
+    def render_job(self, config, width, height, spp, samples_per_frame, threads=0, film=None):
+        """sol::PathTracer driven by sol::RenderJob."""
+        out = _film(width, height, film)
+        cfg = config.to_c()
+        self.lib.ref_renderjob_render(self.h, C.byref(cfg), spp, samples_per_frame, width, height, *_ptrs(out), threads)
+        return out
 
     def trace(self, rays: np.ndarray, any_hit: bool) -> np.ndarray:
         rays = np.ascontiguousarray(rays, np.float32)

@@ -22,6 +22,7 @@
 #include <omp.h>
 
 #include "core/math.h"
+#include "oracle_camera.h"
 #include "sol_gpu.h"
 
 using namespace sol_b200;
@@ -395,7 +396,7 @@ void emission(const Scene& s, uint32_t li, Vec3 dir, Vec2 uv, Rgb* intensity, fl
 // ---------------------------------------------------------------------------
 struct Camera { Vec3 eye, dir, right, up; };
 
-Camera make_camera(const SolGpuCamera& c) {                  // cameras.cpp:5-21
+Camera make_camera(const OracleCamera& c) {                  // cameras.cpp:5-21
     Camera cam;
     cam.eye = ld3(c.eye);
     cam.dir = normalize(ld3(c.dir));
@@ -494,7 +495,7 @@ Scene prepare(const SolGpuSceneDesc* d) {
 extern "C" {
 
 /// PathTracer::render (path_tracer.cpp:9-23) into planar films, `+=` per pixel.
-int oracle_render(const SolGpuSceneDesc* d, const SolGpuCamera* c, const SolGpuConfig* cfg,
+int oracle_render(const SolGpuSceneDesc* d, const OracleCamera* c, const SolGpuConfig* cfg,
                   uint64_t sample_index, uint32_t sample_count, uint32_t w, uint32_t h,
                   float* r, float* g, float* b, int threads) {
     Scene s = prepare(d);

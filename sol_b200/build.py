@@ -22,8 +22,8 @@ LIB_DIR = PKG / "lib"
 BUILD_DIR = PKG / "_build"
 LIB = LIB_DIR / "libsol_gpu.so"
 
-CUDA_SOURCES = ["kernels/megakernel.cu", "kernels/trace.cu"]
-HOST_SOURCES = ["capi.cpp", "host/flatten.cpp"]
+CUDA_SOURCES = ["kernels/megakernel.cu", "kernels/trace.cu", "kernels/wavefront.cu"]
+HOST_SOURCES = ["capi.cpp", "batch.cpp", "host/flatten.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_DEVICE = ARCH + ["-O3", "-lineinfo", "-std=c++20", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",

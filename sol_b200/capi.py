@@ -67,8 +67,7 @@ class SolGpuSceneDesc(C.Structure):
 
 
 class SolGpuCamera(C.Structure):
-    _fields_ = [("eye", C.c_float * 3), ("dir", C.c_float * 3), ("up", C.c_float * 3),
-                ("fov", C.c_float), ("aspect", C.c_float)]
+    _fields_ = [("eye", C.c_float * 3), ("dir", C.c_float * 3), ("right", C.c_float * 3), ("up", C.c_float * 3)]
 
 
 class SolGpuConfig(C.Structure):
@@ -94,7 +93,18 @@ class SolGpuHit(C.Structure):
     _fields_ = [("tri", C.c_int32), ("t", C.c_float), ("u", C.c_float), ("v", C.c_float)]
 
 
+class SolGpuView(C.Structure):
+    _fields_ = [("scene", C.c_uint32), ("camera", SolGpuCamera), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("sample_index", C.c_uint64), ("sample_count", C.c_uint32), ("film", C.c_void_p)]
+
+
+class SolGpuBatchOptions(C.Structure):
+    _fields_ = [("capacity", C.c_uint32), ("block_size", C.c_uint32), ("sort_threshold", C.c_uint32),
+                ("host_loop", C.c_int32)]
+
+
 ScenePtr = C.c_void_p
+BatchPtr = C.c_void_p
 
 # (name, restype, argtypes) of every entry point declared in include/sol_gpu.h
 SIGNATURES = [
@@ -102,6 +112,8 @@ SIGNATURES = [
     ("sol_gpu_abi_version", C.c_int, []),
     ("sol_gpu_device_count", C.c_int, [C.POINTER(C.c_int)]),
     ("sol_gpu_scene_create", C.c_int, [C.POINTER(SolGpuSceneDesc), C.c_int, C.POINTER(ScenePtr)]),
+    ("sol_gpu_camera_perspective", C.c_int, [C.c_float * 3, C.c_float * 3, C.c_float * 3, C.c_float, C.c_float,
+                                             C.POINTER(SolGpuCamera)]),
     ("sol_gpu_scene_destroy", C.c_int, [ScenePtr]),
     ("sol_gpu_scene_info", C.c_int, [ScenePtr, C.POINTER(SolGpuSceneInfo)]),
     ("sol_gpu_render", C.c_int, [ScenePtr, C.POINTER(SolGpuCamera), C.POINTER(SolGpuConfig), C.c_uint64, C.c_uint32,
@@ -111,6 +123,14 @@ SIGNATURES = [
     ("sol_gpu_render_stats", C.c_int, [ScenePtr, C.POINTER(SolGpuRenderStats)]),
     ("sol_gpu_scene_set_instrumented", C.c_int, [ScenePtr, C.c_int]),
     ("sol_gpu_trace", C.c_int, [ScenePtr, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]),
+    ("sol_gpu_batch_create", C.c_int, [C.POINTER(ScenePtr), C.c_uint32, C.POINTER(SolGpuBatchOptions),
+                                       C.POINTER(BatchPtr)]),
+    ("sol_gpu_batch_destroy", C.c_int, [BatchPtr]),
+    ("sol_gpu_batch_render", C.c_int, [BatchPtr, C.POINTER(SolGpuConfig), C.POINTER(SolGpuView), C.c_uint32,
+                                       C.c_void_p]),
+    ("sol_gpu_batch_stats", C.c_int, [BatchPtr, C.POINTER(SolGpuRenderStats)]),
+    ("sol_gpu_batch_autotune", C.c_int, [BatchPtr, C.POINTER(SolGpuConfig), C.POINTER(SolGpuView), C.c_uint32,
+                                         C.c_char_p, C.POINTER(SolGpuBatchOptions)]),
     ("sol_gpu_build_bvh", C.c_int, [f32p, C.c_uint32, u32p, C.c_uint32, C.POINTER(SolGpuBvhNode), u32p, u32p]),
 ]
 

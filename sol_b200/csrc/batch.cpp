@@ -1,0 +1,404 @@
+// Batched wavefront rendering: SolGpuBatch and its C ABI entry points
+// (include/sol_gpu.h), host side.  The stages are in kernels/wavefront.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/sol_gpu.h"
+#include "host/handles.h"
+#include "kernels/wavefront.h"
+
+using namespace sol_b200;
+
+struct SolGpuBatch {
+    int device = 0;
+    int num_sms = 0;
+    std::vector<SolGpuScene*> scenes;
+    SolGpuBatchOptions opts{};
+    uint32_t allocated = 0;           // pool capacity in memory
+    void* pool = nullptr;
+    WfParams host{};                  // host copy of the device parameters
+    WfParams* d_params = nullptr;
+    WfCounters* d_ctr = nullptr;
+    SceneView* d_scenes = nullptr;
+    WfView* d_views = nullptr;
+    size_t views_cap = 0;
+    WfLaunch launch{};
+    int launch_block = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t capture = nullptr;
+    WfCounters* h_ctr = nullptr;      // pinned, for the host-driven loop
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    bool rendered = false;
+};
+
+namespace {
+
+constexpr uint32_t kDefaultCapacity = 1u << 20;
+constexpr uint32_t kMaxCapacity = 1u << 26;
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+size_t pool_bytes(uint32_t c) {
+    size_t b = 0;
+    b += 8 * align256(sizeof(float4) * (size_t)c);                    // ray_o ray_d thru color sum sh_o sh_d pending
+    b += align256(sizeof(unsigned long long) * (size_t)c);            // rng
+    b += align256(sizeof(uint4) * (size_t)c);                         // pix
+    b += align256(sizeof(float2) * (size_t)c);                        // hit
+    b += (4 + kWfBins + 1) * align256(sizeof(uint32_t) * (size_t)c);  // queues
+    return b;
+}
+
+void destroy_graph(SolGpuBatch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+int alloc_pool(SolGpuBatch* b, uint32_t capacity) {
+    if (b->pool && b->allocated >= capacity) return SOL_GPU_OK;
+    destroy_graph(b);
+    cudaFree(b->pool);
+    b->pool = nullptr;
+    b->allocated = 0;
+    cudaError_t e = cudaMalloc(&b->pool, pool_bytes(capacity));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc path pool");
+    b->allocated = capacity;
+    char* p = static_cast<char*>(b->pool);
+    auto take = [&](size_t bytes) { char* r = p; p += align256(bytes); return r; };
+    const size_t c = capacity;
+    WfParams& h = b->host;
+    h.ray_o = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    h.ray_d = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    h.thru = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    h.color = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    h.sum = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    h.sh_o = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    h.sh_d = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    h.pending = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    h.rng = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * c));
+    h.pix = reinterpret_cast<uint4*>(take(sizeof(uint4) * c));
+    h.hit = reinterpret_cast<float2*>(take(sizeof(float2) * c));
+    h.q_extend[0] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
+    h.q_extend[1] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
+    h.q_regen[0] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
+    h.q_regen[1] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
+    h.q_bins = reinterpret_cast<uint32_t*>(p);
+    p += kWfBins * align256(sizeof(uint32_t) * c);
+    h.q_shadow = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
+    return SOL_GPU_OK;
+}
+
+int configure_launch(SolGpuBatch* b) {
+    int block = (int)(b->opts.block_size ? b->opts.block_size : 128);
+    if (block != 64 && block != 128 && block != 256) return fail(SOL_GPU_ERR_INVALID_ARG, "block_size must be 64, 128 or 256");
+    if (block == b->launch_block) return SOL_GPU_OK;
+    for (int s = 0; s < 4; ++s) {
+        int per_sm = wavefront_blocks_per_sm(s, block);
+        if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "wavefront occupancy query failed");
+        b->launch.grid[s] = per_sm * b->num_sms;
+        b->launch.block[s] = block;
+    }
+    b->launch_block = block;
+    destroy_graph(b);
+    return SOL_GPU_OK;
+}
+
+/// Graph = WHILE(condition) { generate, extend, shade, shadow, advance }.
+int build_graph(SolGpuBatch* b) {
+    if (b->exec) return SOL_GPU_OK;
+    cudaError_t e = cudaGraphCreate(&b->graph, 0);
+    cudaGraphConditionalHandle handle{};
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, b->graph, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = handle;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node{};
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, b->graph, nullptr, 0, &np);
+    if (e != cudaSuccess) { destroy_graph(b); return cuda_fail(e, "graph conditional node"); }
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(b->capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        cudaError_t le = launch_wf_iteration(b->d_params, b->launch, handle, 1, b->capture);
+        e = cudaStreamEndCapture(b->capture, &body);
+        if (e == cudaSuccess) e = le;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+    if (e != cudaSuccess) { destroy_graph(b); cudaGetLastError(); return cuda_fail(e, "graph capture"); }
+    return SOL_GPU_OK;
+}
+
+int upload_views(SolGpuBatch* b, const SolGpuView* views, uint32_t n, uint32_t* total_items, uint64_t* pixels,
+                 cudaStream_t stream) {
+    std::vector<WfView> v(n);
+    uint64_t items = 0, px = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const SolGpuView& s = views[i];
+        if (s.scene >= b->scenes.size()) return fail(SOL_GPU_ERR_INVALID_ARG, "view scene index out of range");
+        if (s.width == 0 || s.height == 0) return fail(SOL_GPU_ERR_INVALID_ARG, "view size must be positive");
+        if (!s.film) return fail(SOL_GPU_ERR_INVALID_ARG, "view film must not be NULL");
+        WfView& w = v[i];
+        std::memcpy(w.eye, s.camera.eye, sizeof(w.eye));
+        std::memcpy(w.dir, s.camera.dir, sizeof(w.dir));
+        std::memcpy(w.right, s.camera.right, sizeof(w.right));
+        std::memcpy(w.up, s.camera.up, sizeof(w.up));
+        w.scene = s.scene;
+        w.width = s.width;
+        w.height = s.height;
+        w.sample_count = s.sample_count;
+        w.sample_index = s.sample_index;
+        w.film = s.film;
+        w.tiles_x = (s.width + 7) / 8;
+        w.item_begin = (uint32_t)items;
+        items += (uint64_t)w.tiles_x * ((s.height + 3) / 4) * 32;
+        px += (uint64_t)s.width * s.height;
+        if (items > 0xffffffffull) return fail(SOL_GPU_ERR_INVALID_ARG, "batch too large (more than 2^32 work items)");
+    }
+    if (b->views_cap < n) {
+        cudaFree(b->d_views);
+        b->d_views = nullptr;
+        b->views_cap = 0;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_views), sizeof(WfView) * std::max<size_t>(n, 64));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc views");
+        b->views_cap = std::max<size_t>(n, 64);
+    }
+    cudaError_t e = cudaMemcpyAsync(b->d_views, v.data(), sizeof(WfView) * n, cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "views upload");
+    *total_items = (uint32_t)items;
+    *pixels = px;
+    return SOL_GPU_OK;
+}
+
+int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* views, uint32_t n, cudaStream_t stream) {
+    uint32_t total_items = 0;
+    uint64_t pixels = 0;
+    int rc = upload_views(b, views, n, &total_items, &pixels, stream);
+    if (rc != SOL_GPU_OK) return rc;
+    uint32_t want = b->opts.capacity ? b->opts.capacity : kDefaultCapacity;
+    want = std::min<uint32_t>(std::max<uint32_t>(want, 32), kMaxCapacity);
+    rc = alloc_pool(b, want);
+    if (rc != SOL_GPU_OK) return rc;
+    rc = configure_launch(b);
+    if (rc != SOL_GPU_OK) return rc;
+    WfParams& h = b->host;
+    h.capacity = (uint32_t)std::min<uint64_t>(want, std::max<uint64_t>(pixels, 32));
+    h.sort_threshold = b->opts.sort_threshold;
+    h.num_views = n;
+    h.total_items = total_items;
+    h.cfg = to_config(*config);
+    h.views = b->d_views;
+    h.scenes = b->d_scenes;
+    h.ctr = b->d_ctr;
+    cudaError_t e = cudaMemcpyAsync(b->d_params, &h, sizeof(WfParams), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "params upload");
+    cudaEventRecord(b->ev_start, stream);
+    e = launch_wf_init(b->d_params, h.capacity, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "wavefront init");
+    if (n > 0 && !b->opts.host_loop && build_graph(b) == SOL_GPU_OK) {
+        e = cudaGraphLaunch(b->exec, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+    } else if (n > 0) {
+        // Host-driven loop: the same stages, one iteration per round trip.
+        cudaGraphConditionalHandle none{};
+        for (uint64_t it = 0;; ++it) {
+            e = launch_wf_iteration(b->d_params, b->launch, none, 0, stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_ctr, b->d_ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            if (e != cudaSuccess) return cuda_fail(e, "wavefront iteration");
+            if (!b->h_ctr->more) break;
+        }
+    }
+    cudaEventRecord(b->ev_stop, stream);
+    b->rendered = true;
+    return SOL_GPU_OK;
+}
+
+std::string device_name(int device) {
+    cudaDeviceProp p{};
+    if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return "unknown";
+    return p.name;
+}
+
+std::string tune_key(SolGpuBatch* b, const SolGpuView* views, uint32_t n) {
+    uint64_t px = 0, tris = 0;
+    for (uint32_t i = 0; i < n; ++i) px += (uint64_t)views[i].width * views[i].height;
+    for (auto* s : b->scenes) tris += s->info.num_triangles;
+    std::ostringstream k;
+    k << device_name(b->device) << "|views=" << n << "|px2=" << (int)std::lround(std::log2((double)std::max<uint64_t>(px, 1)))
+      << "|tri2=" << (int)std::lround(std::log2((double)std::max<uint64_t>(tris, 1)));
+    return k.str();
+}
+
+bool read_cache(const char* path, const std::string& key, SolGpuBatchOptions* o) {
+    std::ifstream f(path);
+    std::string line;
+    bool found = false;
+    while (std::getline(f, line)) {
+        std::istringstream in(line);
+        std::string k;
+        SolGpuBatchOptions r{};
+        if (std::getline(in, k, '\t') && (in >> r.capacity >> r.block_size >> r.sort_threshold) && k == key) {
+            *o = r;
+            found = true;
+        }
+    }
+    return found;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sol_gpu_batch_create(SolGpuScene* const* scenes, uint32_t num_scenes, const SolGpuBatchOptions* options,
+                         SolGpuBatch** out) {
+    if (!scenes || num_scenes == 0 || !out) return fail(SOL_GPU_ERR_INVALID_ARG, "scenes and out must not be NULL");
+    *out = nullptr;
+    const int device = scenes[0]->device;
+    for (uint32_t i = 0; i < num_scenes; ++i) {
+        if (!scenes[i]) return fail(SOL_GPU_ERR_INVALID_ARG, "scene must not be NULL");
+        if (scenes[i]->device != device) return fail(SOL_GPU_ERR_INVALID_ARG, "all scenes of a batch must be on one device");
+    }
+    DeviceGuard guard(device);
+    if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
+    auto* b = new SolGpuBatch();
+    b->device = device;
+    b->scenes.assign(scenes, scenes + num_scenes);
+    if (options) b->opts = *options;
+    std::vector<SceneView> views(num_scenes);
+    for (uint32_t i = 0; i < num_scenes; ++i) views[i] = scenes[i]->view;
+    cudaError_t e = cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_params), sizeof(WfParams));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_ctr), sizeof(WfCounters));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_scenes), sizeof(SceneView) * num_scenes);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_scenes, views.data(), sizeof(SceneView) * num_scenes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&b->h_ctr), sizeof(WfCounters));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev_start);
+    if (e == cudaSuccess) e = cudaEventCreate(&b->ev_stop);
+    if (e != cudaSuccess) {
+        int rc = cuda_fail(e, "batch create");
+        sol_gpu_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_batch_destroy(SolGpuBatch* b) {
+    if (!b) return fail(SOL_GPU_ERR_INVALID_ARG, "batch must not be NULL");
+    DeviceGuard guard(b->device);
+    cudaDeviceSynchronize();
+    destroy_graph(b);
+    cudaFree(b->pool);
+    cudaFree(b->d_params);
+    cudaFree(b->d_ctr);
+    cudaFree(b->d_scenes);
+    cudaFree(b->d_views);
+    if (b->h_ctr) cudaFreeHost(b->h_ctr);
+    if (b->capture) cudaStreamDestroy(b->capture);
+    if (b->ev_start) cudaEventDestroy(b->ev_start);
+    if (b->ev_stop) cudaEventDestroy(b->ev_stop);
+    delete b;
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_batch_render(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* views, uint32_t num_views,
+                         void* stream) {
+    if (!b || !config || (num_views > 0 && !views)) return fail(SOL_GPU_ERR_INVALID_ARG, "batch, config and views must not be NULL");
+    DeviceGuard guard(b->device);
+    if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
+    return render_batch(b, config, views, num_views, static_cast<cudaStream_t>(stream));
+}
+
+int sol_gpu_batch_stats(SolGpuBatch* b, SolGpuRenderStats* out) {
+    if (!b || !out) return fail(SOL_GPU_ERR_INVALID_ARG, "batch and out must not be NULL");
+    std::memset(out, 0, sizeof(*out));
+    if (!b->rendered) return SOL_GPU_OK;
+    DeviceGuard guard(b->device);
+    cudaError_t e = cudaEventSynchronize(b->ev_stop);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventSynchronize");
+    WfCounters c;
+    e = cudaMemcpy(&c, b->d_ctr, sizeof(c), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "counters");
+    out->paths = c.paths;
+    out->rays = c.rays;
+    out->shadow_rays = c.shadow_rays;
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop) == cudaSuccess) out->kernel_ms = ms;
+    if (c.error) return fail(SOL_GPU_ERR_BAD_INDEX, "device reported an error");
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* views, uint32_t num_views,
+                           const char* cache_path, SolGpuBatchOptions* chosen) {
+    if (!b || !config || !views || num_views == 0) return fail(SOL_GPU_ERR_INVALID_ARG, "batch, config and views are required");
+    DeviceGuard guard(b->device);
+    if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
+    const std::string key = tune_key(b, views, num_views);
+    SolGpuBatchOptions best = b->opts;
+    if (cache_path && read_cache(cache_path, key, &best)) {
+        best.host_loop = b->opts.host_loop;
+        b->opts = best;
+        if (chosen) *chosen = best;
+        return SOL_GPU_OK;
+    }
+    // Probe: one sample per pixel of every view, into scratch films.
+    std::vector<SolGpuView> probe(views, views + num_views);
+    size_t floats = 0;
+    for (auto& v : probe) floats += 3 * (size_t)v.width * v.height;
+    float* scratch = nullptr;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&scratch), sizeof(float) * std::max<size_t>(floats, 1));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc autotune films");
+    size_t off = 0;
+    for (auto& v : probe) { v.film = scratch + off; off += 3 * (size_t)v.width * v.height; v.sample_count = 1; }
+    cudaStream_t s = b->capture;
+    const uint32_t caps[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21};
+    const uint32_t blocks[] = {64, 128, 256};
+    const uint32_t sorts[] = {0u, 1u << 16, 0xffffffffu};
+    float best_ms = 1e30f;
+    int rc = SOL_GPU_OK;
+    const SolGpuBatchOptions saved = b->opts;
+    for (uint32_t cap : caps) {
+        for (uint32_t blk : blocks) {
+            for (uint32_t srt : sorts) {
+                b->opts.capacity = cap;
+                b->opts.block_size = blk;
+                b->opts.sort_threshold = srt;
+                float ms = 0.0f;
+                for (int rep = 0; rep < 2 && rc == SOL_GPU_OK; ++rep) {   // first run warms the graph
+                    rc = render_batch(b, config, probe.data(), num_views, s);
+                    if (rc == SOL_GPU_OK) {
+                        e = cudaEventSynchronize(b->ev_stop);
+                        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
+                        if (e != cudaSuccess) rc = cuda_fail(e, "autotune timing");
+                    }
+                }
+                if (rc != SOL_GPU_OK) break;
+                if (ms < best_ms) { best_ms = ms; best = b->opts; }
+            }
+        }
+    }
+    cudaFree(scratch);
+    if (rc != SOL_GPU_OK) { b->opts = saved; return rc; }
+    best.host_loop = saved.host_loop;
+    b->opts = best;
+    if (chosen) *chosen = best;
+    if (cache_path) {
+        std::ofstream f(cache_path, std::ios::app);
+        f << key << '\t' << best.capacity << ' ' << best.block_size << ' ' << best.sort_threshold << '\n';
+    }
+    return SOL_GPU_OK;
+}
+
+}  // extern "C"

@@ -10,61 +10,48 @@
 #include "../../include/sol_gpu.h"
 #include "core/layout.h"
 #include "host/flatten.h"
+#include "host/handles.h"
 #include "kernels/kernels.h"
 
 using namespace sol_b200;
 
-struct SolGpuScene {
-    int device = 0;
-    int num_sms = 0;
-    cudaStream_t stream = nullptr;
-    DNode* nodes = nullptr;
-    DTri* tris = nullptr;
-    DTriShade* shade = nullptr;
-    DBsdf* bsdfs = nullptr;
-    DTexture* textures = nullptr;
-    DImage* images = nullptr;
-    float* texels = nullptr;
-    DLight* lights = nullptr;
-    DeviceCounters* counters = nullptr;
-    float* film_tmp = nullptr;       // device film for host-film renders
-    size_t film_tmp_floats = 0;
-    float* film_host = nullptr;      // pinned staging for host-film renders
-    size_t film_host_floats = 0;
-    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
-    bool instrumented = false;
-    bool rendered = false;
-    SceneView view{};
-    SolGpuSceneInfo info{};
-};
+namespace sol_b200 {
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
 int fail(int code, const std::string& msg) {
     g_last_error = msg;
     return code;
 }
 
+const char* last_error() { return g_last_error.c_str(); }
+
 int cuda_fail(cudaError_t e, const char* what) {
     int code = e == cudaErrorMemoryAllocation ? SOL_GPU_ERR_OUT_OF_MEMORY : SOL_GPU_ERR_CUDA;
     return fail(code, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-/// Makes `device` current for the scope of a call and restores the caller's device.
-struct DeviceGuard {
-    int prev = -1;
-    cudaError_t err = cudaSuccess;
-    explicit DeviceGuard(int device) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != device) err = cudaSetDevice(device);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
+DConfig to_config(const SolGpuConfig& c) {
+    DConfig d;
+    d.max_path_len = c.max_path_len;
+    d.min_rr_path_len = c.min_rr_path_len;
+    d.min_survival_prob = c.min_survival_prob;
+    d.max_survival_prob = c.max_survival_prob;
+    d.ray_offset = c.ray_offset;
+    return d;
+}
+
+DCamera to_camera(const SolGpuCamera& c) {
+    DCamera d;
+    for (int k = 0; k < 3; ++k) { d.eye[k] = c.eye[k]; d.dir[k] = c.dir[k]; d.right[k] = c.right[k]; d.up[k] = c.up[k]; }
+    return d;
+}
+
+}  // namespace sol_b200
+
+namespace {
 
 template <typename T>
 cudaError_t upload(T** dst, const std::vector<T>& src) {
@@ -88,16 +75,6 @@ void release(SolGpuScene* s) {
     delete s;
 }
 
-DConfig to_config(const SolGpuConfig& c) {
-    DConfig d;
-    d.max_path_len = c.max_path_len;
-    d.min_rr_path_len = c.min_rr_path_len;
-    d.min_survival_prob = c.min_survival_prob;
-    d.max_survival_prob = c.max_survival_prob;
-    d.ray_offset = c.ray_offset;
-    return d;
-}
-
 int check_render_args(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config,
                       uint32_t width, uint32_t height) {
     if (!scene || !camera || !config) return fail(SOL_GPU_ERR_INVALID_ARG, "scene, camera and config must not be NULL");
@@ -116,7 +93,7 @@ int render_into(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConf
     int per_sm = megakernel_blocks_per_sm(scene->instrumented);
     if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
     int grid = per_sm * scene->num_sms;
-    const DCamera cam = make_camera(*camera);
+    const DCamera cam = to_camera(*camera);
     cudaEventRecord(scene->ev_start, stream);
     e = launch_megakernel(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
                           scene->counters, scene->instrumented, grid, stream);
@@ -130,7 +107,7 @@ int render_into(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConf
 
 extern "C" {
 
-const char* sol_gpu_last_error(void) { return g_last_error.c_str(); }
+const char* sol_gpu_last_error(void) { return sol_b200::last_error(); }
 
 int sol_gpu_abi_version(void) { return SOL_GPU_ABI_VERSION; }
 
@@ -186,6 +163,13 @@ int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** 
                            flat.shade.size() * sizeof(DTriShade);
     s->info.build_ms = (float)flat.build_ms;
     *out = s;
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_camera_perspective(const float eye[3], const float dir[3], const float up[3], float fov, float aspect,
+                               SolGpuCamera* out) {
+    if (!eye || !dir || !up || !out) return fail(SOL_GPU_ERR_INVALID_ARG, "camera arguments must not be NULL");
+    *out = perspective_camera(eye, dir, up, fov, aspect);
     return SOL_GPU_OK;
 }
 

@@ -44,17 +44,17 @@ bvh::Bvh build_mesh_bvh(const float* vertices, const uint32_t* indices, size_t n
     return tree;
 }
 
-DCamera make_camera(const SolGpuCamera& c) {
-    DCamera out;
-    Vec3 dir = normalize(ld3(c.dir));
-    Vec3 right = normalize(cross(ld3(c.dir), ld3(c.up)));
+SolGpuCamera perspective_camera(const float eye[3], const float dir_in[3], const float up_in[3], float fov, float aspect) {
+    SolGpuCamera out;
+    Vec3 dir = normalize(ld3(dir_in));
+    Vec3 right = normalize(cross(ld3(dir_in), ld3(up_in)));
     Vec3 up = cross(right, dir);
-    float w = std::tan(c.fov * std::numbers::pi_v<float> / 360.0f);
-    float h = w / c.aspect;
+    float w = std::tan(fov * std::numbers::pi_v<float> / 360.0f);
+    float h = w / aspect;
     right = right * w;
     up = up * h;
     for (int k = 0; k < 3; ++k) {
-        out.eye[k] = c.eye[k];
+        out.eye[k] = eye[k];
         out.dir[k] = comp(dir, k);
         out.right[k] = comp(right, k);
         out.up[k] = comp(up, k);

@@ -33,6 +33,6 @@ bvh::Bvh build_mesh_bvh(const float* vertices, const uint32_t* indices, size_t n
 bool flatten_scene(const SolGpuSceneDesc& desc, FlatScene& out, std::string& err);
 
 /// PerspectiveCamera's constructor (src/cameras.cpp:5-21).
-DCamera make_camera(const SolGpuCamera& c);
+SolGpuCamera perspective_camera(const float eye[3], const float dir[3], const float up[3], float fov, float aspect);
 
 }  // namespace sol_b200

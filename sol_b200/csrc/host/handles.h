@@ -1,0 +1,64 @@
+// Internal: the scene handle behind SolGpuScene and the status helpers shared
+// by the C ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../../include/sol_gpu.h"
+#include "../core/layout.h"
+
+struct SolGpuScene {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    sol_b200::DNode* nodes = nullptr;
+    sol_b200::DTri* tris = nullptr;
+    sol_b200::DTriShade* shade = nullptr;
+    sol_b200::DBsdf* bsdfs = nullptr;
+    sol_b200::DTexture* textures = nullptr;
+    sol_b200::DImage* images = nullptr;
+    float* texels = nullptr;
+    sol_b200::DLight* lights = nullptr;
+    sol_b200::DeviceCounters* counters = nullptr;
+    float* film_tmp = nullptr;       // device film for host-film renders
+    size_t film_tmp_floats = 0;
+    float* film_host = nullptr;      // pinned staging for host-film renders
+    size_t film_host_floats = 0;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    bool instrumented = false;
+    bool rendered = false;
+    sol_b200::SceneView view{};
+    SolGpuSceneInfo info{};
+};
+
+namespace sol_b200 {
+
+/// Records `msg` as the calling thread's last error and returns `code`.
+int fail(int code, const std::string& msg);
+/// The calling thread's last error message.
+const char* last_error();
+/// Maps a CUDA error to a status code (out-of-memory is reported as such).
+int cuda_fail(cudaError_t e, const char* what);
+
+/// Makes `device` current for the scope of a call and restores the caller's device.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != device) err = cudaSetDevice(device);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+    DeviceGuard(const DeviceGuard&) = delete;
+    DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
+DConfig to_config(const SolGpuConfig& c);
+DCamera to_camera(const SolGpuCamera& c);
+
+}  // namespace sol_b200

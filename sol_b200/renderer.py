@@ -1,0 +1,173 @@
+"""Python mirror of SoL's renderer interface over the C ABI.
+
+  Image          sol::Image with three planar FP32 channels (include/sol/image.h)
+  GpuScene       an uploaded scene (sol_gpu_scene_create / destroy)
+  GpuPathTracer  sol::PathTracer's interface: render(image, sample_index,
+                 sample_count) adds the samples into the image
+                 (include/sol/renderer.h:34, src/algorithms/path_tracer.cpp:9-23)
+
+Every call goes to the CUDA library; failures raise SolGpuError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .scene import Camera, Config, Scene
+
+
+class Image:
+    """sol::Image with 3 channels: planar float32 array of shape (3, height, width)."""
+
+    def __init__(self, width: int, height: int):
+        self.channels = np.zeros((3, height, width), np.float32)
+
+    @property
+    def width(self) -> int:
+        return self.channels.shape[2]
+
+    @property
+    def height(self) -> int:
+        return self.channels.shape[1]
+
+    def clear(self, value: float = 0.0) -> None:       # src/image.cpp:13-16
+        self.channels[...] = np.float32(value)
+
+    def scale(self, value: float) -> None:             # src/image.cpp:18-23
+        self.channels *= np.float32(value)
+
+    def rgb_at(self, x: int, y: int):
+        return tuple(float(self.channels[c, y, x]) for c in range(3))
+
+
+class GpuScene:
+    """A scene uploaded to one GPU. `bvh` optionally passes a prebuilt BVH (see scene.build_bvh)."""
+
+    def __init__(self, scene: Scene, device: int = 0, bvh=None):
+        self.scene = scene
+        self.device = device
+        desc = scene.desc(bvh)
+        h = capi.ScenePtr()
+        capi.check(capi.lib.sol_gpu_scene_create(desc.ptr, device, C.byref(h)), "sol_gpu_scene_create")
+        self.handle = h
+
+    def info(self) -> capi.SolGpuSceneInfo:
+        out = capi.SolGpuSceneInfo()
+        capi.check(capi.lib.sol_gpu_scene_info(self.handle, C.byref(out)), "sol_gpu_scene_info")
+        return out
+
+    def set_instrumented(self, on: bool) -> None:
+        capi.check(capi.lib.sol_gpu_scene_set_instrumented(self.handle, int(on)), "sol_gpu_scene_set_instrumented")
+
+    def trace(self, rays_ptr: int, count: int, any_hit: bool, hits_ptr: int, stream: int = 0) -> None:
+        """Device-pointer batch query (SolGpuRay in, SolGpuHit out)."""
+        capi.check(capi.lib.sol_gpu_trace(self.handle, rays_ptr, count, int(any_hit), hits_ptr, stream), "sol_gpu_trace")
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            capi.check(capi.lib.sol_gpu_scene_destroy(self.handle), "sol_gpu_scene_destroy")
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuPathTracer:
+    """sol::PathTracer on the GPU: same constructor shape (scene, config)."""
+
+    name = "PathTracer"
+
+    def __init__(self, scene: GpuScene | Scene, config: Config | None = None, camera: Camera | None = None,
+                 device: int = 0):
+        self.scene = scene if isinstance(scene, GpuScene) else GpuScene(scene, device)
+        self.config = config or Config()
+        self.camera = camera or self.scene.scene.camera
+        self._cam = self.camera.to_c()
+        self._cfg = self.config.to_c()
+
+    def render(self, image: Image, sample_index: int, sample_count: int = 1) -> None:
+        """Adds samples [sample_index, sample_index + sample_count) of every pixel into `image`."""
+        ch = image.channels
+        if not ch.flags.c_contiguous or ch.dtype != np.float32:
+            raise ValueError("image channels must be C-contiguous float32")
+        f32p = C.POINTER(C.c_float)
+        capi.check(capi.lib.sol_gpu_render(self.scene.handle, C.byref(self._cam), C.byref(self._cfg), sample_index,
+                                           sample_count, image.width, image.height,
+                                           ch[0].ctypes.data_as(f32p), ch[1].ctypes.data_as(f32p),
+                                           ch[2].ctypes.data_as(f32p)), "sol_gpu_render")
+
+    def render_device(self, film_ptr: int, width: int, height: int, sample_index: int, sample_count: int,
+                      stream: int = 0) -> None:
+        """Asynchronous render into a device film of 3*width*height floats (R, G, B planes)."""
+        capi.check(capi.lib.sol_gpu_render_device(self.scene.handle, C.byref(self._cam), C.byref(self._cfg),
+                                                  sample_index, sample_count, width, height, film_ptr, stream),
+                   "sol_gpu_render_device")
+
+    def stats(self) -> capi.SolGpuRenderStats:
+        out = capi.SolGpuRenderStats()
+        capi.check(capi.lib.sol_gpu_render_stats(self.scene.handle, C.byref(out)), "sol_gpu_render_stats")
+        return out
+
+
+class BatchRenderer:
+    """Many views (camera, film, sample range) over one or more GpuScenes in one
+    wavefront launch (sol_gpu_batch_*).  Films are device pointers (3*w*h floats)."""
+
+    def __init__(self, scenes, capacity: int = 0, block_size: int = 0, sort_threshold: int = 0,
+                 host_loop: bool = False):
+        self.scenes = list(scenes)
+        arr = (capi.ScenePtr * len(self.scenes))(*[s.handle for s in self.scenes])
+        opts = capi.SolGpuBatchOptions(capacity, block_size, sort_threshold, int(host_loop))
+        h = capi.BatchPtr()
+        capi.check(capi.lib.sol_gpu_batch_create(arr, len(self.scenes), C.byref(opts), C.byref(h)),
+                   "sol_gpu_batch_create")
+        self.handle = h
+
+    @staticmethod
+    def views(specs) -> "C.Array":
+        """specs: iterable of (scene_index, Camera, width, height, sample_index, sample_count, film_ptr)."""
+        specs = list(specs)
+        arr = (capi.SolGpuView * max(1, len(specs)))()
+        for k, (si, cam, w, h, index, count, film) in enumerate(specs):
+            v = arr[k]
+            v.scene = si
+            v.camera = cam.to_c() if isinstance(cam, Camera) else cam
+            v.width, v.height = w, h
+            v.sample_index, v.sample_count = index, count
+            v.film = film
+        return arr, len(specs)
+
+    def render(self, config: Config, views, stream: int = 0) -> None:
+        arr, n = views
+        cfg = config.to_c()
+        capi.check(capi.lib.sol_gpu_batch_render(self.handle, C.byref(cfg), arr, n, stream), "sol_gpu_batch_render")
+
+    def autotune(self, config: Config, views, cache_path: str | None = None) -> capi.SolGpuBatchOptions:
+        arr, n = views
+        cfg = config.to_c()
+        out = capi.SolGpuBatchOptions()
+        capi.check(capi.lib.sol_gpu_batch_autotune(self.handle, C.byref(cfg), arr, n,
+                                                   cache_path.encode() if cache_path else None, C.byref(out)),
+                   "sol_gpu_batch_autotune")
+        return out
+
+    def stats(self) -> capi.SolGpuRenderStats:
+        out = capi.SolGpuRenderStats()
+        capi.check(capi.lib.sol_gpu_batch_stats(self.handle, C.byref(out)), "sol_gpu_batch_stats")
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            capi.check(capi.lib.sol_gpu_batch_destroy(self.handle), "sol_gpu_batch_destroy")
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

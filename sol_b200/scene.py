@@ -52,12 +52,11 @@ class Camera:
     aspect: float
 
     def to_c(self) -> capi.SolGpuCamera:
+        """The constructed camera (sol_gpu_camera_perspective)."""
         c = capi.SolGpuCamera()
-        c.eye[:] = self.eye
-        c.dir[:] = self.dir
-        c.up[:] = self.up
-        c.fov = self.fov
-        c.aspect = self.aspect
+        v3 = C.c_float * 3
+        capi.check(capi.lib.sol_gpu_camera_perspective(v3(*self.eye), v3(*self.dir), v3(*self.up), self.fov,
+                                                       self.aspect, C.byref(c)), "sol_gpu_camera_perspective")
         return c
 
 
