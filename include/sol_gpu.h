@@ -305,6 +305,61 @@ int sol_gpu_batch_stats(SolGpuBatch* batch, SolGpuRenderStats* out);
 int sol_gpu_batch_autotune(SolGpuBatch* batch, const SolGpuConfig* config, const SolGpuView* views,
                            uint32_t num_views, const char* cache_path, SolGpuBatchOptions* chosen);
 
+/* ---- Differentiation --------------------------------------------------------
+ *
+ * Parameters are the scene's texture values: for each texture in order, a
+ * constant texture's value (1 float) or a constant colour (3 floats), image
+ * textures adding nothing there; then every image's texels (R, G, B planes of
+ * width*height floats) in image order.  They cover SoL's diffuse albedos
+ * (constant or image), Phong specular colours and exponents, mirror and glass
+ * colours, glass ratios, interpolation weights and light emissions.  There is
+ * no SoL counterpart: SoL has no differentiable rendering. */
+
+/* Size of the parameter vector; optionally the offset of each texture's block
+ * (image textures: their image's block) and of each image's block. */
+int sol_gpu_param_layout(const SolGpuScene* scene, uint64_t* count, uint64_t* texture_offsets,
+                         uint64_t* image_offsets);
+
+/* Copies the current parameter values to / from a host vector of `count` floats.
+ * Setting them changes what later renders and adjoints see. */
+int sol_gpu_params_get(const SolGpuScene* scene, float* values);
+int sol_gpu_params_set(SolGpuScene* scene, const float* values);
+
+/* Path-replay adjoint: adds dL/d(parameters) into `grad` (device, `count`
+ * floats) for the paths that sol_gpu_render_device traces with the same camera,
+ * configuration and sample range, given dL/d(film) (device, 3*width*height:
+ * R, G, B planes).  Paths are replayed from their seeds, not stored.
+ * Derivatives reach every colour texture a path's value is linear in (diffuse
+ * albedo, Phong, mirror and glass colours, emission), including the Russian
+ * roulette probability's dependence on the path throughput; scalar textures
+ * (Phong exponent, glass ratio, interpolation weight) receive none here — see
+ * sol_gpu_tangent.  Requires config->max_path_len <= 16.  Asynchronous. */
+int sol_gpu_adjoint(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config,
+                    uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
+                    const float* dl_dfilm, float* grad, void* stream);
+
+/* L2 image loss on the current device: adds sum_i (film_scale * film[i] - target[i])^2
+ * into *loss (a device double) and, when dl_dfilm is not NULL, writes
+ * dL/dfilm[i] = 2 film_scale (film_scale * film[i] - target[i]).  Asynchronous. */
+int sol_gpu_image_l2(const float* film, const float* target, uint64_t count, float film_scale,
+                     float* dl_dfilm, double* loss, void* stream);
+
+/* One view of a fused forward + adjoint batch. */
+typedef struct SolGpuAdjointView {
+    SolGpuView view;       /* camera, size, sample range; the forward sums are added into view.film */
+    const float* target;   /* device, 3*width*height: the loss is sum (sum/sample_count - target)^2 */
+    float* grad;           /* device gradient of the view's scene parameters (added into) */
+    double* loss;          /* device double (added into) */
+} SolGpuAdjointView;
+
+/* Forward render and L2-loss path-replay adjoint of every view, over the batch's
+ * scenes, in one persistent launch: each pixel's samples are rendered (film
+ * bits as sol_gpu_render_device), its loss and loss gradient formed, and the
+ * same samples replayed backwards.  Requires config->max_path_len <= 16.
+ * Asynchronous. */
+int sol_gpu_batch_forward_adjoint(SolGpuBatch* batch, const SolGpuConfig* config, const SolGpuAdjointView* views,
+                                  uint32_t num_views, void* stream);
+
 /* Host-only: builds the BVH that TriangleMesh builds for an indexed mesh
  * (src/triangle_mesh.cpp:119-146: triangle boxes and centroids, full-sweep SAH,
  * reinsertion), in the SolGpuBvhNode form that SolGpuSceneDesc accepts.

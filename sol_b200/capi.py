@@ -98,6 +98,10 @@ class SolGpuView(C.Structure):
                 ("sample_index", C.c_uint64), ("sample_count", C.c_uint32), ("film", C.c_void_p)]
 
 
+class SolGpuAdjointView(C.Structure):
+    _fields_ = [("view", SolGpuView), ("target", C.c_void_p), ("grad", C.c_void_p), ("loss", C.c_void_p)]
+
+
 class SolGpuBatchOptions(C.Structure):
     _fields_ = [("capacity", C.c_uint32), ("block_size", C.c_uint32), ("sort_threshold", C.c_uint32),
                 ("host_loop", C.c_int32)]
@@ -129,8 +133,16 @@ SIGNATURES = [
     ("sol_gpu_batch_render", C.c_int, [BatchPtr, C.POINTER(SolGpuConfig), C.POINTER(SolGpuView), C.c_uint32,
                                        C.c_void_p]),
     ("sol_gpu_batch_stats", C.c_int, [BatchPtr, C.POINTER(SolGpuRenderStats)]),
+    ("sol_gpu_batch_forward_adjoint", C.c_int, [BatchPtr, C.POINTER(SolGpuConfig), C.POINTER(SolGpuAdjointView),
+                                                C.c_uint32, C.c_void_p]),
     ("sol_gpu_batch_autotune", C.c_int, [BatchPtr, C.POINTER(SolGpuConfig), C.POINTER(SolGpuView), C.c_uint32,
                                          C.c_char_p, C.POINTER(SolGpuBatchOptions)]),
+    ("sol_gpu_param_layout", C.c_int, [ScenePtr, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    ("sol_gpu_params_get", C.c_int, [ScenePtr, f32p]),
+    ("sol_gpu_params_set", C.c_int, [ScenePtr, f32p]),
+    ("sol_gpu_adjoint", C.c_int, [ScenePtr, C.POINTER(SolGpuCamera), C.POINTER(SolGpuConfig), C.c_uint64, C.c_uint32,
+                                  C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("sol_gpu_image_l2", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("sol_gpu_build_bvh", C.c_int, [f32p, C.c_uint32, u32p, C.c_uint32, C.POINTER(SolGpuBvhNode), u32p, u32p]),
 ]
 

@@ -13,6 +13,7 @@
 
 #include "../../include/sol_gpu.h"
 #include "host/handles.h"
+#include "kernels/adjoint.h"
 #include "kernels/wavefront.h"
 
 using namespace sol_b200;
@@ -30,6 +31,9 @@ struct SolGpuBatch {
     SceneView* d_scenes = nullptr;
     WfView* d_views = nullptr;
     size_t views_cap = 0;
+    AdjView* d_adj_views = nullptr;
+    size_t adj_views_cap = 0;
+    DeviceCounters* d_fused_ctr = nullptr;
     WfLaunch launch{};
     int launch_block = 0;
     cudaGraph_t graph = nullptr;
@@ -38,6 +42,7 @@ struct SolGpuBatch {
     WfCounters* h_ctr = nullptr;      // pinned, for the host-driven loop
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     bool rendered = false;
+    bool last_fused = false;          // the last launch was sol_gpu_batch_forward_adjoint
 };
 
 namespace {
@@ -221,6 +226,7 @@ int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* v
     }
     cudaEventRecord(b->ev_stop, stream);
     b->rendered = true;
+    b->last_fused = false;
     return SOL_GPU_OK;
 }
 
@@ -305,6 +311,8 @@ int sol_gpu_batch_destroy(SolGpuBatch* b) {
     cudaFree(b->d_ctr);
     cudaFree(b->d_scenes);
     cudaFree(b->d_views);
+    cudaFree(b->d_adj_views);
+    cudaFree(b->d_fused_ctr);
     if (b->h_ctr) cudaFreeHost(b->h_ctr);
     if (b->capture) cudaStreamDestroy(b->capture);
     if (b->ev_start) cudaEventDestroy(b->ev_start);
@@ -321,6 +329,67 @@ int sol_gpu_batch_render(SolGpuBatch* b, const SolGpuConfig* config, const SolGp
     return render_batch(b, config, views, num_views, static_cast<cudaStream_t>(stream));
 }
 
+int sol_gpu_batch_forward_adjoint(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuAdjointView* views,
+                                  uint32_t n, void* stream) {
+    if (!b || !config || (n > 0 && !views)) return fail(SOL_GPU_ERR_INVALID_ARG, "batch, config and views must not be NULL");
+    if (config->max_path_len > (uint32_t)kAdjointMaxDepth)
+        return fail(SOL_GPU_ERR_UNSUPPORTED, "the adjoint replays paths of at most 16 vertices");
+    DeviceGuard guard(b->device);
+    if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    std::vector<AdjView> v(n);
+    uint64_t items = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const SolGpuAdjointView& a = views[i];
+        if (a.view.scene >= b->scenes.size()) return fail(SOL_GPU_ERR_INVALID_ARG, "view scene index out of range");
+        if (a.view.width == 0 || a.view.height == 0 || a.view.sample_count == 0)
+            return fail(SOL_GPU_ERR_INVALID_ARG, "view size and sample count must be positive");
+        if (!a.view.film || !a.target || !a.grad || !a.loss) return fail(SOL_GPU_ERR_INVALID_ARG, "view buffers must not be NULL");
+        AdjView& w = v[i];
+        w.cam = to_camera(a.view.camera);
+        w.scene = a.view.scene;
+        w.width = a.view.width;
+        w.height = a.view.height;
+        w.sample_count = a.view.sample_count;
+        w.sample_index = a.view.sample_index;
+        w.film = a.view.film;
+        w.target = a.target;
+        w.grad = a.grad;
+        w.loss = a.loss;
+        w.item_begin = (uint32_t)items;
+        items += (uint64_t)((a.view.width + 7) / 8) * ((a.view.height + 3) / 4) * 32;
+        if (items > 0xffffffffull) return fail(SOL_GPU_ERR_INVALID_ARG, "batch too large");
+    }
+    cudaError_t e = cudaSuccess;
+    if (b->adj_views_cap < n) {
+        cudaFree(b->d_adj_views);
+        b->d_adj_views = nullptr;
+        b->adj_views_cap = 0;
+        e = cudaMalloc(reinterpret_cast<void**>(&b->d_adj_views), sizeof(AdjView) * std::max<size_t>(n, 32));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc views");
+        b->adj_views_cap = std::max<size_t>(n, 32);
+    }
+    if (!b->d_fused_ctr) {
+        e = cudaMalloc(reinterpret_cast<void**>(&b->d_fused_ctr), sizeof(DeviceCounters));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc counters");
+    }
+    if (n > 0) e = cudaMemcpyAsync(b->d_adj_views, v.data(), sizeof(AdjView) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_fused_ctr, 0, sizeof(DeviceCounters), st);
+    if (e != cudaSuccess) return cuda_fail(e, "fused batch upload");
+    const int per_sm = fused_blocks_per_sm();
+    if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "fused kernel occupancy query failed");
+    cudaEventRecord(b->ev_start, st);
+    if (n > 0) {
+        e = launch_fused_forward_adjoint(b->d_adj_views, n, (uint32_t)items, b->d_scenes, to_config(*config),
+                                         b->d_fused_ctr, per_sm * b->num_sms, st);
+        if (e != cudaSuccess) return cuda_fail(e, "fused forward/adjoint launch");
+    }
+    cudaEventRecord(b->ev_stop, st);
+    b->rendered = true;
+    b->last_fused = true;
+    return SOL_GPU_OK;
+}
+
 int sol_gpu_batch_stats(SolGpuBatch* b, SolGpuRenderStats* out) {
     if (!b || !out) return fail(SOL_GPU_ERR_INVALID_ARG, "batch and out must not be NULL");
     std::memset(out, 0, sizeof(*out));
@@ -328,15 +397,23 @@ int sol_gpu_batch_stats(SolGpuBatch* b, SolGpuRenderStats* out) {
     DeviceGuard guard(b->device);
     cudaError_t e = cudaEventSynchronize(b->ev_stop);
     if (e != cudaSuccess) return cuda_fail(e, "cudaEventSynchronize");
-    WfCounters c;
-    e = cudaMemcpy(&c, b->d_ctr, sizeof(c), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_fail(e, "counters");
-    out->paths = c.paths;
-    out->rays = c.rays;
-    out->shadow_rays = c.shadow_rays;
+    if (b->last_fused) {
+        DeviceCounters c;
+        e = cudaMemcpy(&c, b->d_fused_ctr, sizeof(c), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(e, "counters");
+        out->paths = c.paths;
+        out->rays = c.rays;
+    } else {
+        WfCounters c;
+        e = cudaMemcpy(&c, b->d_ctr, sizeof(c), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(e, "counters");
+        out->paths = c.paths;
+        out->rays = c.rays;
+        out->shadow_rays = c.shadow_rays;
+        if (c.error) return fail(SOL_GPU_ERR_BAD_INDEX, "device reported an error");
+    }
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop) == cudaSuccess) out->kernel_ms = ms;
-    if (c.error) return fail(SOL_GPU_ERR_BAD_INDEX, "device reported an error");
     return SOL_GPU_OK;
 }
 

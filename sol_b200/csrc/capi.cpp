@@ -1,6 +1,7 @@
 // C ABI of the B200 path tracer (include/sol_gpu.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -11,6 +12,7 @@
 #include "core/layout.h"
 #include "host/flatten.h"
 #include "host/handles.h"
+#include "kernels/adjoint.h"
 #include "kernels/kernels.h"
 
 using namespace sol_b200;
@@ -67,7 +69,7 @@ void release(SolGpuScene* s) {
     DeviceGuard g(s->device);
     cudaFree(s->nodes); cudaFree(s->tris); cudaFree(s->shade); cudaFree(s->bsdfs);
     cudaFree(s->textures); cudaFree(s->images); cudaFree(s->texels); cudaFree(s->lights);
-    cudaFree(s->counters); cudaFree(s->film_tmp);
+    cudaFree(s->counters); cudaFree(s->film_tmp); cudaFree(s->param_offsets);
     if (s->film_host) cudaFreeHost(s->film_host);
     if (s->ev_start) cudaEventDestroy(s->ev_start);
     if (s->ev_stop) cudaEventDestroy(s->ev_stop);
@@ -142,6 +144,27 @@ int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** 
     if (e == cudaSuccess) e = upload(&s->texels, flat.texels);
     if (e == cudaSuccess) e = upload(&s->lights, flat.lights);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s->counters), sizeof(DeviceCounters));
+    // Parameter layout: constants in texture order, then the images' texel blocks.
+    s->host_textures = flat.textures;
+    s->host_images = flat.images;
+    s->texel_count = flat.texels.size();
+    uint64_t off = 0;
+    s->texture_offsets.assign(flat.textures.size(), 0);
+    for (size_t i = 0; i < flat.textures.size(); ++i) {
+        const int kind = flat.textures[i].kind;
+        if (kind == SOL_GPU_TEX_CONSTANT) { s->texture_offsets[i] = off; off += 1; }
+        else if (kind == SOL_GPU_TEX_CONSTANT_COLOR) { s->texture_offsets[i] = off; off += 3; }
+    }
+    s->constants_count = off;
+    for (const DImage& im : flat.images) { s->image_offsets.push_back(off + im.offset); }
+    off += flat.texels.size();
+    s->param_count = off;
+    for (size_t i = 0; i < flat.textures.size(); ++i)
+        if (flat.textures[i].kind == SOL_GPU_TEX_IMAGE) s->texture_offsets[i] = s->image_offsets[flat.textures[i].image];
+    {
+        std::vector<unsigned long long> offs(s->texture_offsets.begin(), s->texture_offsets.end());
+        if (e == cudaSuccess) e = upload(&s->param_offsets, offs);
+    }
     if (e != cudaSuccess) { int rc = cuda_fail(e, "scene upload"); release(s); return rc; }
 
     s->view.nodes = s->nodes;
@@ -154,6 +177,7 @@ int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** 
     s->view.lights = s->lights;
     s->view.num_lights = (uint32_t)flat.lights.size();
     s->view.num_tris = desc->num_triangles;
+    s->view.param_offsets = s->param_offsets;
 
     s->info.num_triangles = desc->num_triangles;
     s->info.num_nodes = (uint32_t)flat.nodes.size();
@@ -285,6 +309,83 @@ int sol_gpu_trace(SolGpuScene* scene, const SolGpuRay* rays_device, uint32_t cou
     cudaError_t e = launch_trace(scene->view, rays_device, count, any_hit != 0, hits_device,
                                  static_cast<cudaStream_t>(stream));
     return e == cudaSuccess ? SOL_GPU_OK : cuda_fail(e, "trace launch");
+}
+
+int sol_gpu_param_layout(const SolGpuScene* scene, uint64_t* count, uint64_t* texture_offsets,
+                         uint64_t* image_offsets) {
+    if (!scene || !count) return fail(SOL_GPU_ERR_INVALID_ARG, "scene and count must not be NULL");
+    *count = scene->param_count;
+    if (texture_offsets) std::copy(scene->texture_offsets.begin(), scene->texture_offsets.end(), texture_offsets);
+    if (image_offsets) std::copy(scene->image_offsets.begin(), scene->image_offsets.end(), image_offsets);
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_params_get(const SolGpuScene* scene, float* values) {
+    if (!scene || !values) return fail(SOL_GPU_ERR_INVALID_ARG, "scene and values must not be NULL");
+    for (size_t i = 0; i < scene->host_textures.size(); ++i) {
+        const DTexture& t = scene->host_textures[i];
+        if (t.kind == SOL_GPU_TEX_CONSTANT) values[scene->texture_offsets[i]] = t.v[0];
+        else if (t.kind == SOL_GPU_TEX_CONSTANT_COLOR)
+            for (int c = 0; c < 3; ++c) values[scene->texture_offsets[i] + c] = t.v[c];
+    }
+    if (scene->texel_count == 0) return SOL_GPU_OK;
+    DeviceGuard guard(scene->device);
+    cudaError_t e = cudaMemcpy(values + scene->constants_count, scene->texels, sizeof(float) * scene->texel_count,
+                               cudaMemcpyDeviceToHost);
+    return e == cudaSuccess ? SOL_GPU_OK : cuda_fail(e, "params get");
+}
+
+int sol_gpu_params_set(SolGpuScene* scene, const float* values) {
+    if (!scene || !values) return fail(SOL_GPU_ERR_INVALID_ARG, "scene and values must not be NULL");
+    for (size_t i = 0; i < scene->host_textures.size(); ++i) {
+        DTexture& t = scene->host_textures[i];
+        if (t.kind == SOL_GPU_TEX_CONSTANT) t.v[0] = values[scene->texture_offsets[i]];
+        else if (t.kind == SOL_GPU_TEX_CONSTANT_COLOR)
+            for (int c = 0; c < 3; ++c) t.v[c] = values[scene->texture_offsets[i] + c];
+    }
+    DeviceGuard guard(scene->device);
+    if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
+    cudaError_t e = cudaStreamSynchronize(scene->stream);
+    if (e == cudaSuccess && !scene->host_textures.empty())
+        e = cudaMemcpy(scene->textures, scene->host_textures.data(), sizeof(DTexture) * scene->host_textures.size(),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && scene->texel_count > 0)
+        e = cudaMemcpy(scene->texels, values + scene->constants_count, sizeof(float) * scene->texel_count,
+                       cudaMemcpyHostToDevice);
+    return e == cudaSuccess ? SOL_GPU_OK : cuda_fail(e, "params set");
+}
+
+int sol_gpu_adjoint(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config,
+                    uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
+                    const float* dl_dfilm, float* grad, void* stream) {
+    int rc = check_render_args(scene, camera, config, width, height);
+    if (rc != SOL_GPU_OK) return rc;
+    if (!dl_dfilm || !grad) return fail(SOL_GPU_ERR_INVALID_ARG, "dl_dfilm and grad must not be NULL");
+    if (config->max_path_len > (uint32_t)kAdjointMaxDepth)
+        return fail(SOL_GPU_ERR_UNSUPPORTED, "the adjoint replays paths of at most 16 vertices");
+    DeviceGuard guard(scene->device);
+    if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(scene->counters, 0, sizeof(DeviceCounters), st);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+    const int per_sm = adjoint_blocks_per_sm();
+    if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "adjoint occupancy query failed");
+    cudaEventRecord(scene->ev_start, st);
+    e = launch_adjoint(scene->view, to_camera(*camera), to_config(*config), sample_index, sample_count, width, height,
+                       dl_dfilm, grad, scene->counters, per_sm * scene->num_sms, st);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint launch");
+    cudaEventRecord(scene->ev_stop, st);
+    scene->rendered = true;
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_image_l2(const float* film, const float* target, uint64_t count, float film_scale, float* dl_dfilm,
+                     double* loss, void* stream) {
+    if (!film || !target || !loss) return fail(SOL_GPU_ERR_INVALID_ARG, "film, target and loss must not be NULL");
+    if (count == 0) return SOL_GPU_OK;
+    int grid = (int)std::min<uint64_t>((count + 255) / 256, 4096);
+    cudaError_t e = launch_l2_loss(film, target, count, film_scale, dl_dfilm, loss, grid, static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? SOL_GPU_OK : cuda_fail(e, "loss launch");
 }
 
 int sol_gpu_build_bvh(const float* vertices, uint32_t num_vertices, const uint32_t* indices, uint32_t num_triangles,

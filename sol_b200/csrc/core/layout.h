@@ -104,6 +104,7 @@ struct SceneView {
     const DLight* lights;
     uint32_t num_lights;
     uint32_t num_tris;
+    const unsigned long long* param_offsets;   // per texture, into the parameter vector
 };
 
 /// Per-launch counters and status, zeroed before each launch.

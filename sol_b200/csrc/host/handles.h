@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "../../../include/sol_gpu.h"
 #include "../core/layout.h"
@@ -31,6 +32,15 @@ struct SolGpuScene {
     bool rendered = false;
     sol_b200::SceneView view{};
     SolGpuSceneInfo info{};
+    // Parameter vector (texture values), see sol_gpu_param_layout.
+    std::vector<sol_b200::DTexture> host_textures;
+    std::vector<sol_b200::DImage> host_images;
+    std::vector<uint64_t> texture_offsets;     // per texture (image textures: their image's block)
+    std::vector<uint64_t> image_offsets;       // per image
+    uint64_t param_count = 0;
+    uint64_t constants_count = 0;              // values before the first image block
+    unsigned long long* param_offsets = nullptr;   // device copy of texture_offsets
+    size_t texel_count = 0;
 };
 
 namespace sol_b200 {

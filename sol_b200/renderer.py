@@ -58,6 +58,30 @@ class GpuScene:
         capi.check(capi.lib.sol_gpu_scene_info(self.handle, C.byref(out)), "sol_gpu_scene_info")
         return out
 
+    def param_layout(self):
+        """(count, per-texture offsets, per-image offsets) of the parameter vector."""
+        n = C.c_uint64()
+        capi.check(capi.lib.sol_gpu_param_layout(self.handle, C.byref(n), None, None), "sol_gpu_param_layout")
+        nt, ni = max(1, len(self.scene.textures)), max(1, len(self.scene.images))
+        to = (C.c_uint64 * nt)()
+        io = (C.c_uint64 * ni)()
+        capi.check(capi.lib.sol_gpu_param_layout(self.handle, C.byref(n), to, io), "sol_gpu_param_layout")
+        return n.value, list(to)[:len(self.scene.textures)], list(io)[:len(self.scene.images)]
+
+    def get_params(self) -> np.ndarray:
+        n = self.param_layout()[0]
+        out = np.zeros(n, np.float32)
+        capi.check(capi.lib.sol_gpu_params_get(self.handle, out.ctypes.data_as(C.POINTER(C.c_float))),
+                   "sol_gpu_params_get")
+        return out
+
+    def set_params(self, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, np.float32)
+        if v.size != self.param_layout()[0]:
+            raise ValueError("parameter vector has the wrong size")
+        capi.check(capi.lib.sol_gpu_params_set(self.handle, v.ctypes.data_as(C.POINTER(C.c_float))),
+                   "sol_gpu_params_set")
+
     def set_instrumented(self, on: bool) -> None:
         capi.check(capi.lib.sol_gpu_scene_set_instrumented(self.handle, int(on)), "sol_gpu_scene_set_instrumented")
 
@@ -108,10 +132,24 @@ class GpuPathTracer:
                                                   sample_index, sample_count, width, height, film_ptr, stream),
                    "sol_gpu_render_device")
 
+    def adjoint(self, dl_dfilm_ptr: int, grad_ptr: int, width: int, height: int, sample_index: int,
+                sample_count: int, stream: int = 0) -> None:
+        """Path-replay adjoint: adds dL/d(params) into the device vector at `grad_ptr`."""
+        capi.check(capi.lib.sol_gpu_adjoint(self.scene.handle, C.byref(self._cam), C.byref(self._cfg), sample_index,
+                                            sample_count, width, height, dl_dfilm_ptr, grad_ptr, stream),
+                   "sol_gpu_adjoint")
+
     def stats(self) -> capi.SolGpuRenderStats:
         out = capi.SolGpuRenderStats()
         capi.check(capi.lib.sol_gpu_render_stats(self.scene.handle, C.byref(out)), "sol_gpu_render_stats")
         return out
+
+
+def image_l2(film_ptr: int, target_ptr: int, count: int, film_scale: float, dl_dfilm_ptr: int, loss_ptr: int,
+             stream: int = 0) -> None:
+    """L2 loss kernel: adds sum (s*film - target)^2 into the device double at loss_ptr."""
+    capi.check(capi.lib.sol_gpu_image_l2(film_ptr, target_ptr, count, film_scale, dl_dfilm_ptr or None, loss_ptr,
+                                         stream), "sol_gpu_image_l2")
 
 
 class BatchRenderer:
@@ -146,6 +184,22 @@ class BatchRenderer:
         arr, n = views
         cfg = config.to_c()
         capi.check(capi.lib.sol_gpu_batch_render(self.handle, C.byref(cfg), arr, n, stream), "sol_gpu_batch_render")
+
+    def forward_adjoint(self, config: Config, specs, stream: int = 0) -> None:
+        """Fused forward + L2-loss adjoint. specs: (scene_index, Camera, w, h, sample_index, sample_count,
+        film_ptr, target_ptr, grad_ptr, loss_ptr) per view, all device pointers."""
+        specs = list(specs)
+        arr = (capi.SolGpuAdjointView * max(1, len(specs)))()
+        for k, (si, cam, w, h, index, count, film, target, grad, loss) in enumerate(specs):
+            a = arr[k]
+            a.view.scene = si
+            a.view.camera = cam.to_c() if isinstance(cam, Camera) else cam
+            a.view.width, a.view.height = w, h
+            a.view.sample_index, a.view.sample_count = index, count
+            a.view.film, a.target, a.grad, a.loss = film, target, grad, loss
+        cfg = config.to_c()
+        capi.check(capi.lib.sol_gpu_batch_forward_adjoint(self.handle, C.byref(cfg), arr, len(specs), stream),
+                   "sol_gpu_batch_forward_adjoint")
 
     def autotune(self, config: Config, views, cache_path: str | None = None) -> capi.SolGpuBatchOptions:
         arr, n = views

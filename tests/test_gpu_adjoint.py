@@ -1,0 +1,207 @@
+"""Path-replay adjoint against central finite differences with common random
+numbers, on the textured Cornell box of the adjoint configuration (two RGB
+albedo images on the back wall and floor, constant albedos, Phong specular
+colour and light emission).
+
+The forward render and the adjoint are wrapped in a torch.autograd.Function;
+the loss is L2 between the 16-spp render and a target rendered from other
+textures.  Finite differences use eps = 1e-3 and the same sample indices, on
+the GPU forward and, for a subset, on SoL's own CPU renderer.  Tolerance: the
+relative error of the gradient vector over the checked parameters is at most 2%."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+W = H = 64
+SPP = 8
+EPS = 1e-3
+
+
+def _setup(tex_size=64, seed=0):
+    import torch
+    from sol_b200 import scenes
+    from sol_b200.renderer import GpuPathTracer, GpuScene
+    truth = scenes.cornell_box(0, textured=True, tex_size=tex_size, tex_seed=3)
+    start = scenes.cornell_box(0, textured=True, tex_size=tex_size, tex_seed=11)
+    cfg = scenes.CORNELL_CONFIG
+    gt = GpuScene(truth)
+    target = torch.zeros((3, H, W), device="cuda")
+    GpuPathTracer(gt, cfg).render_device(target.data_ptr(), W, H, 10_000, 64, torch.cuda.current_stream().cuda_stream)
+    target /= 64
+    gs = GpuScene(start)
+    return start, gs, GpuPathTracer(gs, cfg), target
+
+
+class Render:
+    """torch.autograd.Function over sol_gpu_render_device / sol_gpu_adjoint."""
+
+    @staticmethod
+    def make(pt, scene, spp, index):
+        import torch
+
+        class Fn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, params):
+                scene.set_params(params.detach().cpu().numpy())
+                film = torch.zeros((3, H, W), device="cuda")
+                pt.render_device(film.data_ptr(), W, H, index, spp, torch.cuda.current_stream().cuda_stream)
+                ctx.n = params.numel()
+                return film / spp
+
+            @staticmethod
+            def backward(ctx, grad_image):
+                dl_dfilm = (grad_image / spp).contiguous()
+                grad = torch.zeros(ctx.n, device="cuda")
+                pt.adjoint(dl_dfilm.data_ptr(), grad.data_ptr(), W, H, index, spp, torch.cuda.current_stream().cuda_stream)
+                return grad
+
+        return Fn.apply
+
+
+def _loss_np(img, target):
+    d = img.astype(np.float64) - target.astype(np.float64)
+    return float(np.sum(d * d))
+
+
+def _choose(gs, n_texels, seed):
+    count, tex_off, img_off = gs.param_layout()
+    rng = np.random.default_rng(seed)
+    consts = [tex_off[1] + 0, tex_off[2] + 1, tex_off[0] + 2, tex_off[4] + 0, tex_off[4] + 1, tex_off[7] + 2,
+              tex_off[3] + 1]                     # red, green, white albedo; emission r, g; phong ks b; light surface
+    texels = list(rng.choice(np.arange(img_off[0], count), size=n_texels, replace=False))
+    return consts + [int(t) for t in texels]
+
+
+def test_adjoint_matches_gpu_finite_differences(built):
+    import torch
+    scene, gs, pt, target = _setup()
+    params0 = torch.from_numpy(gs.get_params()).cuda()
+    fn = Render.make(pt, gs, SPP, 0)
+    p = params0.clone().requires_grad_(True)
+    loss = ((fn(p) - target) ** 2).sum()
+    loss.backward()
+    g_adj = p.grad.cpu().numpy()
+    idx = _choose(gs, 57, seed=1)
+    tgt = target.cpu().numpy()
+    g_fd = []
+    for i in idx:
+        vals = []
+        for sgn in (1.0, -1.0):
+            q = params0.clone()
+            q[i] += sgn * EPS
+            vals.append(_loss_np(fn(q).cpu().numpy(), tgt))
+        g_fd.append((vals[0] - vals[1]) / (2 * EPS))
+    g_fd = np.array(g_fd)
+    ga = g_adj[idx]
+    rel = np.linalg.norm(ga - g_fd) / np.linalg.norm(g_fd)
+    print("adjoint vs GPU FD: relative error", rel)
+    assert rel <= 0.02
+    gs.set_params(params0.cpu().numpy())
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="SoL's sources are not built here")
+def test_adjoint_matches_sol_cpu_finite_differences(built):
+    """Finite differences of SoL's own PathTracer (CPU) on the constants and a few texels."""
+    import torch
+    from sol_b200 import scenes
+    scene, gs, pt, target = _setup(tex_size=32)
+    params0 = gs.get_params()
+    fn = Render.make(pt, gs, SPP, 0)
+    p = torch.from_numpy(params0).cuda().requires_grad_(True)
+    ((fn(p) - target) ** 2).sum().backward()
+    g_adj = p.grad.cpu().numpy()
+    count, tex_off, img_off = gs.param_layout()
+    tgt = target.cpu().numpy()
+
+    def cpu_loss(values):
+        s = scenes.cornell_box(0, textured=True, tex_size=32, tex_seed=11)
+        for t, off in zip(s.textures, tex_off):
+            if t.type == 1:
+                t.value = tuple(float(x) for x in values[off:off + 3])
+            elif t.type == 0:
+                t.value = (float(values[off]), 0.0, 0.0)
+        s.images = [values[o:o + 3 * 32 * 32].reshape(3, 32, 32).copy() for o in img_off]
+        film, _ = oracle.RefScene(s).render(scenes.CORNELL_CONFIG, W, H, SPP, sample_index=0)
+        return _loss_np(film / SPP, tgt)
+
+    idx = _choose(gs, 5, seed=2)[:10]
+    g_fd = []
+    for i in idx:
+        hi = params0.copy(); hi[i] += EPS
+        lo = params0.copy(); lo[i] -= EPS
+        g_fd.append((cpu_loss(hi) - cpu_loss(lo)) / (2 * EPS))
+    g_fd = np.array(g_fd)
+    rel = np.linalg.norm(g_adj[idx] - g_fd) / np.linalg.norm(g_fd)
+    print("adjoint vs SoL CPU FD: relative error", rel)
+    assert rel <= 0.02
+
+
+def test_loss_kernel_matches_numpy(built):
+    import torch
+    from sol_b200.renderer import image_l2
+    rng = np.random.default_rng(0)
+    a = torch.from_numpy(rng.random((3, 50, 70), dtype=np.float32)).cuda()
+    b = torch.from_numpy(rng.random((3, 50, 70), dtype=np.float32)).cuda()
+    g = torch.zeros_like(a)
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    image_l2(a.data_ptr(), b.data_ptr(), a.numel(), 0.5, g.data_ptr(), loss.data_ptr())
+    torch.cuda.synchronize()
+    d = 0.5 * a.cpu().numpy().astype(np.float64) - b.cpu().numpy()
+    assert abs(loss.item() - np.sum(d * d)) <= 1e-9 * np.sum(d * d)
+    assert np.allclose(g.cpu().numpy(), 2 * 0.5 * d, rtol=1e-5, atol=1e-6)
+
+
+def test_params_roundtrip(built):
+    from sol_b200 import scenes
+    from sol_b200.renderer import GpuScene
+    s = scenes.cornell_box(0, textured=True, tex_size=16)
+    gs = GpuScene(s)
+    v = gs.get_params()
+    count, tex_off, img_off = gs.param_layout()
+    assert v.size == count == 7 * 3 + 2 + 2 * 3 * 16 * 16   # 7 colours, 2 scalars, 2 images
+    assert np.array_equal(v[img_off[0]:img_off[0] + 3 * 256].reshape(3, 16, 16), s.images[0])
+    v2 = v.copy()
+    v2[tex_off[0]:tex_off[0] + 3] = 0.5
+    gs.set_params(v2)
+    assert np.array_equal(gs.get_params(), v2)
+
+
+def test_fused_batch_forward_adjoint_matches_separate_kernels(built):
+    """One launch over views of two scenes: films equal the megakernel's bit for bit,
+    losses and gradients equal the separate adjoint's (up to atomic summation order)."""
+    import torch
+    from sol_b200 import scenes
+    from sol_b200.renderer import BatchRenderer, GpuPathTracer, GpuScene
+    sa = scenes.cornell_box(0, textured=True, tex_size=32)
+    sb = scenes.cornell_box(1, textured=True, tex_size=16, tex_seed=7)
+    ga, gb = GpuScene(sa), GpuScene(sb)
+    cfg = scenes.CORNELL_CONFIG
+    stream = torch.cuda.current_stream().cuda_stream
+    views = [(0, sa.camera, 40, 24, 3, 4), (1, sb.camera, 24, 32, 100, 2), (0, sa.camera, 16, 16, 9, 3)]
+    targets = [torch.rand((3, h, w), device="cuda") * 0.5 for (_, _, w, h, _, _) in views]
+    films = [torch.zeros((3, h, w), device="cuda") for (_, _, w, h, _, _) in views]
+    grads = [torch.zeros(g.param_layout()[0], device="cuda") for g in (ga, gb)]
+    losses = torch.zeros(len(views), dtype=torch.float64, device="cuda")
+    br = BatchRenderer([ga, gb])
+    br.forward_adjoint(cfg, [(si, cam, w, h, idx, spp, f.data_ptr(), t.data_ptr(), grads[si].data_ptr(),
+                              losses[k:k + 1].data_ptr())
+                             for k, ((si, cam, w, h, idx, spp), f, t) in enumerate(zip(views, films, targets))], stream)
+    torch.cuda.synchronize()
+    ref_grads = [torch.zeros_like(g) for g in grads]
+    for k, ((si, cam, w, h, idx, spp), f, t) in enumerate(zip(views, films, targets)):
+        pt = GpuPathTracer((ga, gb)[si], cfg, camera=cam)
+        film = torch.zeros((3, h, w), device="cuda")
+        pt.render_device(film.data_ptr(), w, h, idx, spp, stream)
+        torch.cuda.synchronize()
+        assert torch.equal(film, f)
+        d = film / spp - t
+        assert abs(losses[k].item() - float((d.double() ** 2).sum())) <= 1e-6 * max(1.0, losses[k].item())
+        dl = (2 * d / spp).contiguous()
+        pt.adjoint(dl.data_ptr(), ref_grads[si].data_ptr(), w, h, idx, spp, stream)
+    torch.cuda.synchronize()
+    for g, r in zip(grads, ref_grads):
+        assert torch.allclose(g, r, rtol=1e-4, atol=1e-6)
+        assert float(r.abs().sum()) > 0
