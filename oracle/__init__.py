@@ -70,6 +70,11 @@ def oracle_lib() -> C.CDLL:
         lib.oracle_trace.restype = C.c_int
         lib.oracle_pcg_floats.argtypes = [C.c_uint64, C.c_uint32, f32p]
         lib.oracle_pcg_floats.restype = None
+        lib.oracle_debug_path.argtypes = [C.POINTER(capi.SolGpuSceneDesc), C.POINTER(CameraArgs),
+                                          C.POINTER(capi.SolGpuConfig), C.c_uint64, C.c_uint32, C.c_uint32,
+                                          C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                          C.POINTER(C.c_float)]
+        lib.oracle_debug_path.restype = C.c_uint32
         lib.oracle_pixel_seeds.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
         lib.oracle_pixel_seeds.restype = None
         _oracle = lib
@@ -137,6 +142,21 @@ def trace(scene, rays: np.ndarray, any_hit: bool) -> np.ndarray:
     hits = np.zeros((rays.shape[0], 4), np.float32)
     oracle_lib().oracle_trace(desc.ptr, rays.ctypes.data, rays.shape[0], int(any_hit), hits.ctypes.data)
     return hits
+
+
+def debug_path(scene, config, frame: int, x: int, y: int, width: int, height: int, camera=None, cap: int = 64):
+    """Rays of one (pixel, sample) path: (rays (n, 8), kinds (n,), hits (n, 4), colour (3,))."""
+    desc = scene.desc()
+    cam = camera_args(camera or scene.camera)
+    cfg = config.to_c()
+    rays = np.zeros((cap, 8), np.float32)
+    kinds = np.zeros(cap, np.int32)
+    hits = np.zeros((cap, 4), np.float32)
+    col = (C.c_float * 3)()
+    n = oracle_lib().oracle_debug_path(desc.ptr, C.byref(cam), C.byref(cfg), frame, x, y, width, height,
+                                       rays.ctypes.data, kinds.ctypes.data, hits.ctypes.data, cap, col)
+    n = min(n, cap)
+    return rays[:n], kinds[:n], hits[:n], np.array(list(col), np.float32)
 
 
 def pcg_floats(seed: int, n: int) -> np.ndarray:

@@ -409,7 +409,23 @@ Camera make_camera(const OracleCamera& c) {                  // cameras.cpp:5-21
     return cam;
 }
 
-Rgb trace_path(const Scene& s, const SolGpuConfig& cfg, Sampler& sampler, Vec3 org, Vec3 dir, float tmin) {
+/// Optional record of the rays one path traces (for debugging divergences).
+struct PathLog {
+    SolGpuRay* rays;     // extension and shadow rays in trace order
+    int32_t* kinds;      // 0 = extension, 1 = shadow
+    SolGpuHit* hits;     // result of each ray (shadow: tri >= 0 when occluded)
+    uint32_t cap, n;
+    void add(int kind, Vec3 o, Vec3 d, float t0, float t1, bool hit, const Hit& h) {
+        if (!rays || n >= cap) { ++n; return; }
+        rays[n] = SolGpuRay{{o.x, o.y, o.z}, t0, {d.x, d.y, d.z}, t1};
+        kinds[n] = kind;
+        hits[n] = hit ? SolGpuHit{(int32_t)h.tri, h.t, h.u, h.v} : SolGpuHit{-1, 0.0f, 0.0f, 0.0f};
+        ++n;
+    }
+};
+
+Rgb trace_path(const Scene& s, const SolGpuConfig& cfg, Sampler& sampler, Vec3 org, Vec3 dir, float tmin,
+               PathLog* log = nullptr) {
     const uint32_t nl = s.d->num_lights;
     const float light_pick_prob = 1.0f / (float)nl;
     float pdf_prev_bounce = 0.0f;
@@ -417,7 +433,9 @@ Rgb trace_path(const Scene& s, const SolGpuConfig& cfg, Sampler& sampler, Vec3 o
     Rgb color = rgb(0.0f);
     for (uint32_t path_len = 0; path_len < cfg.max_path_len; path_len++) {
         Hit hit;
-        if (!cast(s, org, dir, tmin, kFloatMax, false, &hit)) break;
+        const bool found = cast(s, org, dir, tmin, kFloatMax, false, &hit);
+        if (log) log->add(0, org, dir, tmin, kFloatMax, found, hit);
+        if (!found) break;
         const float tmax = hit.t;
         SurfaceInfo si = surface(s, hit, org, dir);
         int32_t light = s.d->tri_light[hit.tri];
@@ -442,7 +460,9 @@ Rgb trace_path(const Scene& s, const SolGpuConfig& cfg, Sampler& sampler, Vec3 o
                 Vec3 in_dir = ls.pos - si.point;
                 float cos_surf = dot(in_dir, si.normal());
                 Hit occ;
-                if (!cast(s, si.point, ls.pos - si.point, cfg.ray_offset, 1.0f - cfg.ray_offset, true, &occ)) {
+                const bool occluded = cast(s, si.point, ls.pos - si.point, cfg.ray_offset, 1.0f - cfg.ray_offset, true, &occ);
+                if (log) log->add(1, si.point, ls.pos - si.point, cfg.ray_offset, 1.0f - cfg.ray_offset, occluded, occ);
+                if (!occluded) {
                     float inv_light_dist = 1.0f / length(in_dir);
                     cos_surf *= inv_light_dist;
                     in_dir = in_dir * inv_light_dist;
@@ -537,6 +557,25 @@ int oracle_trace(const SolGpuSceneDesc* d, const SolGpuRay* rays, uint32_t count
         hits[i] = o;
     }
     return 0;
+}
+
+/// Replays one (pixel, sample) path and records its rays, hits and colour.
+/// Returns the number of rays the path traced (records beyond `cap` are dropped).
+uint32_t oracle_debug_path(const SolGpuSceneDesc* d, const OracleCamera* c, const SolGpuConfig* cfg, uint64_t frame,
+                           uint32_t x, uint32_t y, uint32_t w, uint32_t h, SolGpuRay* rays, int32_t* kinds,
+                           SolGpuHit* hits, uint32_t cap, float* color) {
+    Scene s = prepare(d);
+    Camera cam = make_camera(*c);
+    Sampler sampler(pixel_seed(frame, x, (uint64_t)y));
+    float ry = sampler();
+    float rx = sampler();
+    float u = ((float)x + rx) * (2.0f / (float)w) - 1.0f;
+    float v = 1.0f - ((float)y + ry) * (2.0f / (float)h);
+    Vec3 dir = normalize(cam.dir + u * cam.right + v * cam.up);
+    PathLog log{rays, kinds, hits, cap, 0};
+    Rgb col = trace_path(s, *cfg, sampler, cam.eye, dir, 0.0f, &log);
+    color[0] = col.r; color[1] = col.g; color[2] = col.b;
+    return log.n;
 }
 
 /// `n` consecutive draws of PcgSampler(seed) in call order.

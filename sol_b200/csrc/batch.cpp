@@ -201,6 +201,13 @@ int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* v
     h.sort_threshold = b->opts.sort_threshold;
     h.num_views = n;
     h.total_items = total_items;
+    {
+        // Bound on bounce iterations: every sample of every pixel, each vertex plus its start.
+        unsigned long long work = 0;
+        for (uint32_t i = 0; i < n; ++i)
+            work += (unsigned long long)views[i].width * views[i].height * ((unsigned long long)views[i].sample_count + 1ull);
+        h.max_iterations = work * ((unsigned long long)config->max_path_len + 2ull) + 16ull;
+    }
     h.cfg = to_config(*config);
     h.views = b->d_views;
     h.scenes = b->d_scenes;
@@ -222,6 +229,7 @@ int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* v
             if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
             if (e != cudaSuccess) return cuda_fail(e, "wavefront iteration");
             if (!b->h_ctr->more) break;
+            if (it > h.max_iterations) return fail(SOL_GPU_ERR_TIMEOUT, "bounce loop exceeded its bound");
         }
     }
     cudaEventRecord(b->ev_stop, stream);
@@ -410,10 +418,14 @@ int sol_gpu_batch_stats(SolGpuBatch* b, SolGpuRenderStats* out) {
         out->paths = c.paths;
         out->rays = c.rays;
         out->shadow_rays = c.shadow_rays;
-        if (c.error) return fail(SOL_GPU_ERR_BAD_INDEX, "device reported an error");
+        if (c.error) return fail(SOL_GPU_ERR_BAD_INDEX, "a wavefront self-check failed (flags " + std::to_string(c.error) + ")");
     }
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop) == cudaSuccess) out->kernel_ms = ms;
+    for (SolGpuScene* sc : b->scenes) {
+        int rc = check_fault(sc);
+        if (rc != SOL_GPU_OK) return rc;
+    }
     return SOL_GPU_OK;
 }
 

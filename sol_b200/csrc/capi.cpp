@@ -45,6 +45,21 @@ DConfig to_config(const SolGpuConfig& c) {
     return d;
 }
 
+int check_fault(SolGpuScene* s) {
+    unsigned int f = 0;
+    cudaError_t e = cudaMemcpy(&f, s->fault, sizeof(f), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "fault read");
+    if (f == 0) return SOL_GPU_OK;
+    cudaMemset(s->fault, 0, sizeof(unsigned int));
+    std::string msg = "a kernel self-check failed:";
+    if (f & kFaultTraversalSteps) msg += " traversal exceeded its step bound or stack;";
+    if (f & kFaultNodeIndex) msg += " BVH node index out of range;";
+    if (f & kFaultTriIndex) msg += " triangle index out of range;";
+    if (f & kFaultPathLoop) msg += " render loop exceeded its bound;";
+    if (f & kFaultClaimLoop) msg += " pixel claim loop exceeded its bound;";
+    return fail(SOL_GPU_ERR_BAD_INDEX, msg);
+}
+
 DCamera to_camera(const SolGpuCamera& c) {
     DCamera d;
     for (int k = 0; k < 3; ++k) { d.eye[k] = c.eye[k]; d.dir[k] = c.dir[k]; d.right[k] = c.right[k]; d.up[k] = c.up[k]; }
@@ -69,7 +84,7 @@ void release(SolGpuScene* s) {
     DeviceGuard g(s->device);
     cudaFree(s->nodes); cudaFree(s->tris); cudaFree(s->shade); cudaFree(s->bsdfs);
     cudaFree(s->textures); cudaFree(s->images); cudaFree(s->texels); cudaFree(s->lights);
-    cudaFree(s->counters); cudaFree(s->film_tmp); cudaFree(s->param_offsets);
+    cudaFree(s->counters); cudaFree(s->film_tmp); cudaFree(s->param_offsets); cudaFree(s->fault);
     if (s->film_host) cudaFreeHost(s->film_host);
     if (s->ev_start) cudaEventDestroy(s->ev_start);
     if (s->ev_stop) cudaEventDestroy(s->ev_stop);
@@ -144,6 +159,8 @@ int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** 
     if (e == cudaSuccess) e = upload(&s->texels, flat.texels);
     if (e == cudaSuccess) e = upload(&s->lights, flat.lights);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s->counters), sizeof(DeviceCounters));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&s->fault), sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(s->fault, 0, sizeof(unsigned int));
     // Parameter layout: constants in texture order, then the images' texel blocks.
     s->host_textures = flat.textures;
     s->host_images = flat.images;
@@ -178,6 +195,9 @@ int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** 
     s->view.num_lights = (uint32_t)flat.lights.size();
     s->view.num_tris = desc->num_triangles;
     s->view.param_offsets = s->param_offsets;
+    s->view.num_nodes = (uint32_t)flat.nodes.size();
+    s->view.max_steps = (uint32_t)std::min<uint64_t>(2ull * (flat.nodes.size() + flat.tris.size()) + 16ull, 0xffffffffull);
+    s->view.fault = s->fault;
 
     s->info.num_triangles = desc->num_triangles;
     s->info.num_nodes = (uint32_t)flat.nodes.size();
@@ -265,6 +285,8 @@ int sol_gpu_render(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuC
     e = cudaMemcpyAsync(scene->film_host, scene->film_tmp, floats * sizeof(float), cudaMemcpyDeviceToHost, scene->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(scene->stream);
     if (e != cudaSuccess) return cuda_fail(e, "render");
+    rc = check_fault(scene);
+    if (rc != SOL_GPU_OK) return rc;
     // Image::accumulate: one add per pixel and channel (include/sol/image.h:54-60).
     const float* src = scene->film_host;
     float* dst[3] = {film_r, film_g, film_b};
@@ -291,8 +313,7 @@ int sol_gpu_render_stats(SolGpuScene* scene, SolGpuRenderStats* out) {
     out->tris_tested = c.tris;
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, scene->ev_start, scene->ev_stop) == cudaSuccess) out->kernel_ms = ms;
-    if (c.error) return fail(SOL_GPU_ERR_BAD_INDEX, "device reported an error");
-    return SOL_GPU_OK;
+    return check_fault(scene);
 }
 
 int sol_gpu_trace(SolGpuScene* scene, const SolGpuRay* rays_device, uint32_t count, int any_hit,

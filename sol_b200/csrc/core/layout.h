@@ -105,6 +105,18 @@ struct SceneView {
     uint32_t num_lights;
     uint32_t num_tris;
     const unsigned long long* param_offsets;   // per texture, into the parameter vector
+    uint32_t num_nodes;
+    uint32_t max_steps;      // bound on traversal loop iterations (a tree never needs more)
+    unsigned int* fault;     // device word; kernels OR kFault* bits into it instead of looping or reading out of bounds
+};
+
+/// Bits a kernel records in SceneView::fault when a self-check fails.
+enum : unsigned int {
+    kFaultTraversalSteps = 1u,   // a traversal exceeded max_steps
+    kFaultNodeIndex = 2u,        // a node reference outside the node array
+    kFaultTriIndex = 4u,         // a triangle slot outside the triangle array
+    kFaultPathLoop = 8u,         // a render loop exceeded its iteration bound
+    kFaultClaimLoop = 16u,       // the pixel-claim loop exceeded its iteration bound
 };
 
 /// Per-launch counters and status, zeroed before each launch.

@@ -23,6 +23,7 @@ struct SolGpuScene {
     float* texels = nullptr;
     sol_b200::DLight* lights = nullptr;
     sol_b200::DeviceCounters* counters = nullptr;
+    unsigned int* fault = nullptr;   // kFault* bits set by the kernels' self-checks
     float* film_tmp = nullptr;       // device film for host-film renders
     size_t film_tmp_floats = 0;
     float* film_host = nullptr;      // pinned staging for host-film renders
@@ -69,6 +70,10 @@ struct DeviceGuard {
 };
 
 DConfig to_config(const SolGpuConfig& c);
+
+/// Reads (and clears) the fault word of a scene after its work finished;
+/// returns SOL_GPU_OK or an error describing the failed self-check.
+int check_fault(SolGpuScene* s);
 DCamera to_camera(const SolGpuCamera& c);
 
 }  // namespace sol_b200

@@ -186,7 +186,7 @@ __device__ void adjoint_path(const SceneView& s, const DConfig& cfg, const DCame
     for (uint32_t path_len = 0; path_len < cfg.max_path_len && K < kAdjointMaxDepth; ++path_len) {
         float t = kFloatMax;
         TraversalCounters tc{0u, 0u};
-        const int slot = traverse<false, false>(s.nodes, s.tris, ps.org, ps.dir, ps.tmin, t, s.num_tris > 0, tc);
+        const int slot = traverse<false, false>(s, ps.org, ps.dir, ps.tmin, t, tc);
         ++n_rays;
         if (slot < 0) break;
         VertexRec& R = rec[K++];
@@ -224,8 +224,7 @@ __device__ void adjoint_path(const SceneView& s, const DConfig& cfg, const DCame
                 Vec3 in_dir = ls.pos - sf.point;
                 float cos_surf = dot(in_dir, sf.normal());
                 float smax = 1.0f - cfg.ray_offset;
-                const int occ = traverse<true, false>(s.nodes, s.tris, sf.point, ls.pos - sf.point, cfg.ray_offset,
-                                                      smax, s.num_tris > 0, tc);
+                const int occ = traverse<true, false>(s, sf.point, ls.pos - sf.point, cfg.ray_offset, smax, tc);
                 ++n_rays;
                 if (occ < 0) {
                     const float inv_light_dist = 1.0f / length(in_dir);
@@ -378,15 +377,14 @@ fused_forward_adjoint(const AdjView* __restrict__ views, uint32_t num_views, uin
             for (uint32_t len = 0; len < cfg.max_path_len; ++len) {
                 float t = kFloatMax;
                 TraversalCounters tc{0u, 0u};
-                const int slot = traverse<false, false>(s.nodes, s.tris, ps.org, ps.dir, ps.tmin, t, s.num_tris > 0, tc);
+                const int slot = traverse<false, false>(s, ps.org, ps.dir, ps.tmin, t, tc);
                 ++n_rays;
                 if (slot < 0) break;
                 VertexOut vo;
                 shade_vertex(s, cfg, light_pick_prob, slot, t, ps, vo);
                 if (vo.has_shadow) {
                     float smax = 1.0f - cfg.ray_offset;
-                    const int occ = traverse<true, false>(s.nodes, s.tris, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax,
-                                                          s.num_tris > 0, tc);
+                    const int occ = traverse<true, false>(s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc);
                     ++n_rays;
                     if (occ < 0) ps.color = ps.color + vo.pending;
                 }

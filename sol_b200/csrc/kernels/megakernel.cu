@@ -48,7 +48,6 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
     const uint32_t total = tiles_x * ((height + 3u) / 4u) * 32u;
     const size_t plane = (size_t)width * height;
     const float light_pick_prob = 1.0f / (float)s.num_lights;
-    const bool has_geometry = s.num_tris > 0;
 
     TraversalCounters tc{0u, 0u};
     uint32_t n_paths = 0, n_rays = 0, n_shadow = 0;
@@ -58,11 +57,18 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
     Rgb pix_sum = rgb(0.0f);
     PathState ps;
     bool done = false;
+    // Self-check bounds: a lane never needs more iterations than the pixels it
+    // can claim times their samples times the path length (plus one per claim).
+    const unsigned long long loop_bound = (unsigned long long)total * ((unsigned long long)sample_count + 1ull) *
+                                          ((unsigned long long)cfg.max_path_len + 1ull) + 64ull;
+    unsigned long long iterations = 0, claims = 0;
+    bool alive = false;   // the lane has a path in flight
 
     while (true) {
+        if (++iterations > loop_bound) { atomicOr(s.fault, kFaultPathLoop); break; }
         // --- make sure this lane has a live path (or stop) ------------------
-        bool alive = false;
         while (!alive) {
+            if (++claims > loop_bound) { atomicOr(s.fault, kFaultClaimLoop); done = true; break; }
             if (have_pixel && sample < sample_count) {
                 start_path(ps, cam, sample_index + sample, px, py, width, height);
                 ++n_paths;
@@ -93,7 +99,7 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
 
         // --- closest hit (path_tracer.cpp:42) ------------------------------
         float t = kFloatMax;
-        const int slot = traverse<false, kCount>(s.nodes, s.tris, ps.org, ps.dir, ps.tmin, t, has_geometry, tc);
+        const int slot = traverse<false, kCount>(s, ps.org, ps.dir, ps.tmin, t, tc);
         ++n_rays;
 
         VertexOut vo;
@@ -104,8 +110,7 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
         // --- shadow ray of this vertex (path_tracer.cpp:72-74) -------------
         if (vo.has_shadow) {
             float smax = 1.0f - cfg.ray_offset;
-            const int occ = traverse<true, kCount>(s.nodes, s.tris, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax,
-                                                   has_geometry, tc);
+            const int occ = traverse<true, kCount>(s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc);
             ++n_rays;
             ++n_shadow;
             if (occ < 0) ps.color = ps.color + vo.pending;
@@ -119,6 +124,7 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
         if (end) {
             pix_sum = pix_sum + ps.color;   // path_tracer.cpp:19
             ++sample;
+            alive = false;
         }
     }
 

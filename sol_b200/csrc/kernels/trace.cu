@@ -21,7 +21,7 @@ trace_rays(SceneView s, const SolGpuRay* __restrict__ rays, uint32_t count, SolG
     const Vec3 org = vec3(a.x, a.y, a.z), dir = vec3(b.x, b.y, b.z);
     float tmax = b.w;
     TraversalCounters tc{0u, 0u};
-    const int slot = traverse<kAnyHit, false>(s.nodes, s.tris, org, dir, a.w, tmax, true, tc);
+    const int slot = traverse<kAnyHit, false>(s, org, dir, a.w, tmax, tc);
     SolGpuHit h;
     h.tri = -1; h.t = 0.0f; h.u = 0.0f; h.v = 0.0f;
     if (slot >= 0) {

@@ -7,10 +7,11 @@
 // traversal is the stack-based "while-while" loop of Aila & Laine ("Understanding
 // the Efficiency of Ray Traversal on GPUs", HPG 2009): descend inner nodes
 // nearest-child first, pushing the farther child, until a leaf is reached; then
-// test the leaf's triangles.  Box tests use one FMA per slab and widen the exit
-// distance by kSlabWiden so that they are conservative; the triangle test is
-// the shared watertight test, so a hit found here is bit-identical to the one the
-// host checker finds.
+// test the leaf's triangles.  Box tests compute (bound - origin) / direction and
+// widen the exit distance by kSlabWiden so that they are conservative; they are
+// the same operations as the host traversal's, so both visit children in the same
+// order and resolve equal-distance hits alike.  The triangle test is the shared
+// watertight test, so a hit found here is bit-identical to the one the host finds.
 #pragma once
 
 #include "../core/layout.h"
@@ -31,15 +32,20 @@ __device__ __forceinline__ Vec3 tri_vertex(float4 a) { return vec3(a.x, a.y, a.z
 /// (tmin, tmax) is returned; otherwise the closest one, with `tmax` shrunk to
 /// its distance.  Returns the triangle's position in leaf order, or -1.
 /// `active == false` lanes return -1 at once but keep the warp convergent.
+/// Self-checks: the loop runs at most `max_steps` iterations, node and
+/// triangle references are checked against the array sizes and the stack
+/// against its capacity; a failed check ORs a kFault* bit into `*fault` and ends
+/// the traversal (no out-of-bounds access, no unbounded loop).
 template <bool kAnyHit, bool kCount>
-__device__ __forceinline__ int traverse(const DNode* __restrict__ nodes, const DTri* __restrict__ tris,
+__device__ __forceinline__ int traverse_bounded(const DNode* __restrict__ nodes, const DTri* __restrict__ tris,
                                         Vec3 org, Vec3 dir, float tmin, float& tmax, bool active,
-                                        TraversalCounters& ctr) {
+                                        TraversalCounters& ctr, uint32_t num_nodes, uint32_t num_tris,
+                                        uint32_t max_steps, unsigned int* fault) {
     int stack[kTraversalStack];
     int sp = 0;
     int hit = -1;
+    uint32_t steps = 0;
     const Vec3 idir = safe_inverse(dir);
-    const Vec3 ood = vec3(-org.x * idir.x, -org.y * idir.y, -org.z * idir.z);
     const RayShear rs = make_shear(org, dir);
     int node = active ? 0 : kStackSentinel;
     stack[sp++] = kStackSentinel;
@@ -47,18 +53,23 @@ __device__ __forceinline__ int traverse(const DNode* __restrict__ nodes, const D
     while (node != kStackSentinel) {
         // Descend inner nodes until a leaf (or the end) is reached.
         while (node >= 0) {
+            if (++steps > max_steps) { atomicOr(fault, kFaultTraversalSteps); return -1; }
+            if ((uint32_t)node >= num_nodes) { atomicOr(fault, kFaultNodeIndex); return -1; }
             const DNode* n = nodes + node;
             const float4 a = ldg4(n->b0);
             const float4 b = ldg4(n->b1);
             const float4 c = ldg4(n->b2);
             const int4 r = __ldg(reinterpret_cast<const int4*>(n->ref));
             if (kCount) ctr.nodes++;
-            float t0lx = __fmaf_rn(a.x, idir.x, ood.x), t0hx = __fmaf_rn(a.y, idir.x, ood.x);
-            float t0ly = __fmaf_rn(a.z, idir.y, ood.y), t0hy = __fmaf_rn(a.w, idir.y, ood.y);
-            float t0lz = __fmaf_rn(c.x, idir.z, ood.z), t0hz = __fmaf_rn(c.y, idir.z, ood.z);
-            float t1lx = __fmaf_rn(b.x, idir.x, ood.x), t1hx = __fmaf_rn(b.y, idir.x, ood.x);
-            float t1ly = __fmaf_rn(b.z, idir.y, ood.y), t1hy = __fmaf_rn(b.w, idir.y, ood.y);
-            float t1lz = __fmaf_rn(c.z, idir.z, ood.z), t1hz = __fmaf_rn(c.w, idir.z, ood.z);
+            // (bound - org) * (1/dir): two correctly rounded operations per plane, so the
+            // widened exit distance stays conservative even for grazing rays (the
+            // product-with-offset form loses |org / dir| ulps to cancellation).
+            float t0lx = (a.x - org.x) * idir.x, t0hx = (a.y - org.x) * idir.x;
+            float t0ly = (a.z - org.y) * idir.y, t0hy = (a.w - org.y) * idir.y;
+            float t0lz = (c.x - org.z) * idir.z, t0hz = (c.y - org.z) * idir.z;
+            float t1lx = (b.x - org.x) * idir.x, t1hx = (b.y - org.x) * idir.x;
+            float t1ly = (b.z - org.y) * idir.y, t1hy = (b.w - org.y) * idir.y;
+            float t1lz = (c.z - org.z) * idir.z, t1hz = (c.w - org.z) * idir.z;
             float n0 = fmaxf(fmaxf(fminf(t0lx, t0hx), fminf(t0ly, t0hy)), fmaxf(fminf(t0lz, t0hz), tmin));
             float f0 = fminf(fminf(fmaxf(t0lx, t0hx), fmaxf(t0ly, t0hy)), fminf(fmaxf(t0lz, t0hz), tmax)) * kSlabWiden;
             float n1 = fmaxf(fmaxf(fminf(t1lx, t1hx), fminf(t1ly, t1hy)), fmaxf(fminf(t1lz, t1hz), tmin));
@@ -67,6 +78,7 @@ __device__ __forceinline__ int traverse(const DNode* __restrict__ nodes, const D
             if (h0 && h1) {
                 int near = r.x, far = r.y;
                 if (n1 < n0) { near = r.y; far = r.x; }
+                if (sp >= kTraversalStack) { atomicOr(fault, kFaultTraversalSteps); return -1; }
                 stack[sp++] = far;
                 node = near;
             } else if (h0) {
@@ -74,6 +86,7 @@ __device__ __forceinline__ int traverse(const DNode* __restrict__ nodes, const D
             } else if (h1) {
                 node = r.y;
             } else {
+                if (sp <= 0) { atomicOr(fault, kFaultTraversalSteps); return -1; }
                 node = stack[--sp];
             }
         }
@@ -81,6 +94,8 @@ __device__ __forceinline__ int traverse(const DNode* __restrict__ nodes, const D
         // Leaf: ~node = (first << 3) | (count - 1)
         const uint32_t v = ~(uint32_t)node;
         const uint32_t first = v >> 3, count = (v & 7u) + 1u;
+        if (first + count > num_tris) { atomicOr(fault, kFaultTriIndex); return -1; }
+        if (++steps > max_steps) { atomicOr(fault, kFaultTraversalSteps); return -1; }
         for (uint32_t i = first; i < first + count; ++i) {
             const DTri* tp = tris + i;
             const float4 p0 = ldg4(tp->v0), p1 = ldg4(tp->v1), p2 = ldg4(tp->v2);
@@ -93,9 +108,18 @@ __device__ __forceinline__ int traverse(const DNode* __restrict__ nodes, const D
             }
         }
         if (kAnyHit && hit >= 0) break;
+        if (sp <= 0) { atomicOr(fault, kFaultTraversalSteps); return -1; }
         node = stack[--sp];
     }
     return hit;
+}
+
+/// traverse_bounded over the arrays and limits of a scene view.
+template <bool kAnyHit, bool kCount>
+__device__ __forceinline__ int traverse(const SceneView& s, Vec3 org, Vec3 dir, float tmin, float& tmax,
+                                        TraversalCounters& ctr) {
+    return traverse_bounded<kAnyHit, kCount>(s.nodes, s.tris, org, dir, tmin, tmax, s.num_tris > 0, ctr, s.num_nodes,
+                                             s.num_tris, s.max_steps, s.fault);
 }
 
 }  // namespace sol_b200

@@ -56,9 +56,11 @@ __device__ __forceinline__ uint32_t append_keyed(uint32_t* counters, int key) {
 
 __device__ __forceinline__ uint32_t claim(uint32_t* counter) { return append(counter); }
 
+/// Sum over the whole warp; every lane of the block must call it (the stage
+/// kernels have no early exits, so all lanes reach their final reduction).
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
-    const unsigned mask = __activemask();
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(mask, v, off);
+    __syncwarp();
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     return v;
 }
 
@@ -139,7 +141,9 @@ __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ 
             px.w += 1;
         }
         bool started = false;
+        uint32_t claims = 0;
         while (!started) {
+            if (++claims > total + 2u) { atomicOr(&ctr->error, kFaultClaimLoop); break; }
             if (px.x != kIdle) {
                 const WfView& v = P.views[px.x];
                 if (px.w < v.sample_count) {
@@ -197,8 +201,7 @@ __global__ void __launch_bounds__(256) wf_extend(const WfParams* __restrict__ Pp
         const SceneView& sv = P.scenes[P.views[P.pix[slot].x].scene];
         float t = kFloatMax;
         TraversalCounters tc{0u, 0u};
-        const int hit = traverse<false, false>(sv.nodes, sv.tris, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, t,
-                                               sv.num_tris > 0, tc);
+        const int hit = traverse<false, false>(sv, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, t, tc);
         ++rays;
         if (hit < 0) {
             P.q_regen[p ^ 1u][append(&ctr->regen[p ^ 1u])] = slot;
@@ -268,8 +271,7 @@ __global__ void __launch_bounds__(256) wf_shadow(const WfParams* __restrict__ Pp
         const SceneView& sv = P.scenes[P.views[P.pix[slot].x].scene];
         float smax = 1.0f - offset;
         TraversalCounters tc{0u, 0u};
-        const int occ = traverse<true, false>(sv.nodes, sv.tris, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), offset, smax,
-                                              sv.num_tris > 0, tc);
+        const int occ = traverse<true, false>(sv, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), offset, smax, tc);
         ++rays;
         if (occ < 0) {
             const float4 c = P.color[slot];
@@ -292,7 +294,8 @@ __global__ void wf_advance(const WfParams* __restrict__ Pp, cudaGraphConditional
     for (int b = 0; b < kWfBins; ++b) c->bins[b] = 0;
     c->shadow = 0;
     c->iter += 1;
-    const bool more = c->extend[p ^ 1u] + c->regen[p ^ 1u] > 0;
+    bool more = c->extend[p ^ 1u] + c->regen[p ^ 1u] > 0;
+    if (more && c->iter >= P.max_iterations) { c->error |= kFaultPathLoop; more = false; }
     c->more = more ? 1u : 0u;
     if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
 }

@@ -43,6 +43,7 @@ struct WfParams {
     uint32_t sort_threshold;
     uint32_t num_views;
     uint32_t total_items;
+    unsigned long long max_iterations;   // self-check bound on bounce-loop iterations
     DConfig cfg;
     const WfView* views;
     const SceneView* scenes;
