@@ -269,9 +269,11 @@ def run_ours(args):
     peak, peak_src = load_peaks()
     achieved = alg_bytes / (kernel_s / args.steps) / 1e9
     traffic = None
-    tfile = ROOT / "profiles" / "megakernel_sphere_field_traffic.json"
+    tfile = ROOT / "profiles" / "megakernel_sphere_field_traffic.txt"
     if tfile.exists() and not args.small:
-        traffic = json.loads(tfile.read_text()).get("dram_bytes_per_launch")
+        for line in tfile.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch:"):
+                traffic = float(line.split(":", 1)[1])
     line = None
     if rank == 0:
         line = {

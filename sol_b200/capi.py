@@ -9,7 +9,10 @@ from __future__ import annotations
 import ctypes as C
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libsol_gpu.so"
+import os
+
+# SOL_B200_LIBRARY selects another build of the library (e.g. a tuning variant).
+LIB_PATH = Path(os.environ.get("SOL_B200_LIBRARY") or Path(__file__).resolve().parent / "lib" / "libsol_gpu.so")
 
 OK = 0
 ERR_INVALID_ARG = -1

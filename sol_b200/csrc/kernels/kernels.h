@@ -9,7 +9,16 @@
 
 namespace sol_b200 {
 
-constexpr int kMegakernelBlock = 128;
+#ifndef SOL_MEGAKERNEL_BLOCK
+#define SOL_MEGAKERNEL_BLOCK 128
+#endif
+#ifndef SOL_MEGAKERNEL_MIN_BLOCKS
+#define SOL_MEGAKERNEL_MIN_BLOCKS 8   // 64 registers: measured fastest despite spills (latency-bound traversal)
+#endif
+/// Threads per block of the megakernel, and the resident blocks per SM its
+/// register allocation must allow (the compile-time occupancy target).
+constexpr int kMegakernelBlock = SOL_MEGAKERNEL_BLOCK;
+constexpr int kMegakernelMinBlocks = SOL_MEGAKERNEL_MIN_BLOCKS;
 constexpr int kTraceBlock = 128;
 
 /// Resident blocks per SM of the megakernel (for sizing its persistent grid).

@@ -41,7 +41,7 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 }
 
 template <bool kCount>
-__global__ void __launch_bounds__(kMegakernelBlock)
+__global__ void __launch_bounds__(kMegakernelBlock, kMegakernelMinBlocks)
 pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint32_t sample_count,
               uint32_t width, uint32_t height, float* __restrict__ film, DeviceCounters* __restrict__ ctr) {
     const uint32_t tiles_x = (width + 7u) / 8u;
