@@ -360,6 +360,28 @@ typedef struct SolGpuAdjointView {
 int sol_gpu_batch_forward_adjoint(SolGpuBatch* batch, const SolGpuConfig* config, const SolGpuAdjointView* views,
                                   uint32_t num_views, void* stream);
 
+/* The launch of sol_gpu_batch_forward_adjoint for callers that must not
+ * allocate device memory while they render: a host that owns the device-memory
+ * budget and forbids libraries to call cudaMalloc, or a loop that cannot
+ * afford the device synchronisation of cudaFree.  No counterpart in the
+ * reference (SoL renders on the CPU and has no device memory).
+ *
+ * It takes the scenes directly (no SolGpuBatch, whose creation allocates);
+ * view.scene indexes `scenes`.  It allocates nothing: its scene table, view
+ * table and counters live in a fixed 63,744-byte array inside the library, one
+ * per GPU.  At most 64 scenes (all on one device) and 512 views per call;
+ * larger calls fail with SOL_GPU_ERR_INVALID_ARG and say so in
+ * sol_gpu_last_error.  Results are those of sol_gpu_batch_forward_adjoint:
+ * films, gradients and losses are added into (the caller clears them); the
+ * counters in the array are cleared by the call itself.  Calls share the
+ * array, so calls that can overlap on the GPU (different streams without
+ * ordering, different host threads) race: order them.  The first call on a
+ * device looks up the array's address; make it before any stream capture.
+ * Requires config->max_path_len <= 16.  Asynchronous. */
+int sol_gpu_batch_forward_adjoint_noalloc(SolGpuScene* const* scenes, uint32_t num_scenes,
+                                          const SolGpuConfig* config, const SolGpuAdjointView* views,
+                                          uint32_t num_views, void* stream);
+
 /* Host-only: builds the BVH that TriangleMesh builds for an indexed mesh
  * (src/triangle_mesh.cpp:119-146: triangle boxes and centroids, full-sweep SAH,
  * reinsertion), in the SolGpuBvhNode form that SolGpuSceneDesc accepts.

@@ -22,7 +22,8 @@ LIB_DIR = PKG / "lib"
 BUILD_DIR = PKG / "_build"
 LIB = LIB_DIR / "libsol_gpu.so"
 
-CUDA_SOURCES = ["kernels/megakernel.cu", "kernels/trace.cu", "kernels/wavefront.cu", "kernels/adjoint.cu"]
+CUDA_SOURCES = ["kernels/megakernel.cu", "kernels/trace.cu", "kernels/wavefront.cu", "kernels/adjoint.cu",
+                "noalloc.cu"]
 HOST_SOURCES = ["capi.cpp", "batch.cpp", "host/flatten.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -138,6 +138,8 @@ SIGNATURES = [
     ("sol_gpu_batch_stats", C.c_int, [BatchPtr, C.POINTER(SolGpuRenderStats)]),
     ("sol_gpu_batch_forward_adjoint", C.c_int, [BatchPtr, C.POINTER(SolGpuConfig), C.POINTER(SolGpuAdjointView),
                                                 C.c_uint32, C.c_void_p]),
+    ("sol_gpu_batch_forward_adjoint_noalloc", C.c_int, [C.POINTER(ScenePtr), C.c_uint32, C.POINTER(SolGpuConfig),
+                                                        C.POINTER(SolGpuAdjointView), C.c_uint32, C.c_void_p]),
     ("sol_gpu_batch_autotune", C.c_int, [BatchPtr, C.POINTER(SolGpuConfig), C.POINTER(SolGpuView), C.c_uint32,
                                          C.c_char_p, C.POINTER(SolGpuBatchOptions)]),
     ("sol_gpu_param_layout", C.c_int, [ScenePtr, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
