@@ -47,6 +47,11 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--small", action="store_true", help="quick run on a reduced frame (not a bench number)")
+    p.add_argument("--workload", default="frame", choices=["frame", "views", "adjoint", "scenes"],
+                   help="frame: one large frame, plain megakernel (default); views: 64 uneven views of a "
+                        "4,194,314-triangle field, batched wavefront vs 64 plain launches; adjoint: path-replay "
+                        "adjoint vs forward on the textured Cornell box; scenes: fused forward + adjoint over 32 "
+                        "independent scenes")
     return p.parse_args()
 
 
@@ -314,6 +319,14 @@ def run_ours(args):
 
 def main():
     args = parse()
+    if args.workload != "frame":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the CPU reference arm covers the frame workload"}))
+            return 0
+        if dist_env()[1] > 1:
+            raise SystemExit("the views/adjoint/scenes workloads run on one GPU")
+        import bench_workloads
+        return bench_workloads.run(args, ClockSampler, load_peaks)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

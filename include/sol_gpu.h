@@ -246,6 +246,18 @@ int sol_gpu_render_stats(SolGpuScene* scene, SolGpuRenderStats* out);
  * bytes per ray). */
 int sol_gpu_scene_set_instrumented(SolGpuScene* scene, int instrumented);
 
+/* Render schedules of sol_gpu_render / sol_gpu_render_device.  Both give the
+ * same film bits.  PER_PIXEL: one lane renders all samples of a pixel.  SPLIT:
+ * every (pixel, sample) is a work item and the samples are summed per pixel in
+ * order afterwards (uses scratch memory of 12 bytes per pixel and sample, at
+ * most 256 MiB, held by the scene handle; renders through one handle must
+ * therefore be ordered, e.g. issued on one stream).  AUTO (the default) picks
+ * SPLIT for images with fewer pixels than twice the resident lanes. */
+#define SOL_GPU_SCHEDULE_AUTO      0
+#define SOL_GPU_SCHEDULE_PER_PIXEL 1
+#define SOL_GPU_SCHEDULE_SPLIT     2
+int sol_gpu_scene_set_schedule(SolGpuScene* scene, int schedule);
+
 /* Closest-hit (any_hit == 0) or any-hit (any_hit != 0) queries for a batch of
  * device-resident rays, the device side of TriangleMesh::intersect_closest /
  * intersect_any (src/triangle_mesh.cpp:64-117).  Asynchronous on `stream`. */
@@ -331,9 +343,12 @@ int sol_gpu_params_set(SolGpuScene* scene, const float* values);
  * R, G, B planes).  Paths are replayed from their seeds, not stored.
  * Derivatives reach every colour texture a path's value is linear in (diffuse
  * albedo, Phong, mirror and glass colours, emission), including the Russian
- * roulette probability's dependence on the path throughput; scalar textures
- * (Phong exponent, glass ratio, interpolation weight) receive none here — see
- * sol_gpu_tangent.  Requires config->max_path_len <= 16.  Asynchronous. */
+ * roulette probability's dependence on the path throughput.  Phong exponents
+ * receive the derivative of the BSDF value with sampling detached (sampled
+ * directions, pdfs and MIS weights held fixed): unbiased for the derivative of
+ * the expected image, but not the per-sample derivative a finite difference
+ * with common random numbers measures.  Glass ratios and interpolation weights
+ * receive none.  Requires config->max_path_len <= 16.  Asynchronous. */
 int sol_gpu_adjoint(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config,
                     uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
                     const float* dl_dfilm, float* grad, void* stream);

@@ -23,6 +23,7 @@ ERR_QUEUE_OVERFLOW = -5
 ERR_BAD_INDEX = -6
 ERR_UNSUPPORTED = -7
 ERR_CANCELLED = -8
+SCHEDULE_AUTO, SCHEDULE_PER_PIXEL, SCHEDULE_SPLIT = 0, 1, 2
 
 BSDF_DIFFUSE, BSDF_PHONG, BSDF_MIRROR, BSDF_GLASS, BSDF_INTERP = range(5)
 TEX_CONSTANT, TEX_CONSTANT_COLOR, TEX_IMAGE = range(3)
@@ -129,6 +130,7 @@ SIGNATURES = [
                                         C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("sol_gpu_render_stats", C.c_int, [ScenePtr, C.POINTER(SolGpuRenderStats)]),
     ("sol_gpu_scene_set_instrumented", C.c_int, [ScenePtr, C.c_int]),
+    ("sol_gpu_scene_set_schedule", C.c_int, [ScenePtr, C.c_int]),
     ("sol_gpu_trace", C.c_int, [ScenePtr, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]),
     ("sol_gpu_batch_create", C.c_int, [C.POINTER(ScenePtr), C.c_uint32, C.POINTER(SolGpuBatchOptions),
                                        C.POINTER(BatchPtr)]),

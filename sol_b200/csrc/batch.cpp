@@ -365,7 +365,8 @@ int sol_gpu_batch_forward_adjoint(SolGpuBatch* b, const SolGpuConfig* config, co
         w.grad = a.grad;
         w.loss = a.loss;
         w.item_begin = (uint32_t)items;
-        items += (uint64_t)((a.view.width + 7) / 8) * ((a.view.height + 3) / 4) * 32;
+        w.group = fused_group(a.view.sample_count);
+        items += fused_items(a.view.width, a.view.height, a.view.sample_count);
         if (items > 0xffffffffull) return fail(SOL_GPU_ERR_INVALID_ARG, "batch too large");
     }
     cudaError_t e = cudaSuccess;

@@ -84,7 +84,7 @@ void release(SolGpuScene* s) {
     DeviceGuard g(s->device);
     cudaFree(s->nodes); cudaFree(s->tris); cudaFree(s->shade); cudaFree(s->bsdfs);
     cudaFree(s->textures); cudaFree(s->images); cudaFree(s->texels); cudaFree(s->lights);
-    cudaFree(s->counters); cudaFree(s->film_tmp); cudaFree(s->param_offsets); cudaFree(s->fault);
+    cudaFree(s->counters); cudaFree(s->film_tmp); cudaFree(s->split_scratch); cudaFree(s->param_offsets); cudaFree(s->fault);
     if (s->film_host) cudaFreeHost(s->film_host);
     if (s->ev_start) cudaEventDestroy(s->ev_start);
     if (s->ev_stop) cudaEventDestroy(s->ev_stop);
@@ -111,9 +111,32 @@ int render_into(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConf
     if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
     int grid = per_sm * scene->num_sms;
     const DCamera cam = to_camera(*camera);
+    // Split schedule when the image has fewer than two pixels per resident lane
+    // and its per-sample colours fit in a modest scratch buffer.
+    const uint64_t lanes = (uint64_t)grid * kMegakernelBlock;
+    const uint64_t pixels = (uint64_t)width * height;
+    const uint64_t items = (uint64_t)((width + 7) / 8) * ((height + 3) / 4) * 32 * sample_count;
+    const uint64_t scratch_floats = 3 * pixels * sample_count;
+    const bool fits = items < 0x80000000ull && scratch_floats * sizeof(float) <= kSplitScratchMaxBytes;
+    if (scene->schedule == SOL_GPU_SCHEDULE_SPLIT && !fits)
+        return fail(SOL_GPU_ERR_UNSUPPORTED, "the split schedule needs more than 256 MiB of scratch for this render");
+    const bool split = scene->schedule == SOL_GPU_SCHEDULE_SPLIT ||
+                       (scene->schedule == SOL_GPU_SCHEDULE_AUTO && sample_count > 1 && pixels < 2 * lanes && fits);
+    if (split && scene->split_floats < scratch_floats) {
+        cudaFree(scene->split_scratch);
+        scene->split_scratch = nullptr;
+        scene->split_floats = 0;
+        e = cudaMalloc(reinterpret_cast<void**>(&scene->split_scratch), scratch_floats * sizeof(float));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc split scratch");
+        scene->split_floats = scratch_floats;
+    }
     cudaEventRecord(scene->ev_start, stream);
-    e = launch_megakernel(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
-                          scene->counters, scene->instrumented, grid, stream);
+    if (split)
+        e = launch_megakernel_split(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
+                                    scene->split_scratch, scene->counters, scene->instrumented, grid, stream);
+    else
+        e = launch_megakernel(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
+                              scene->counters, scene->instrumented, grid, stream);
     if (e != cudaSuccess) return cuda_fail(e, "megakernel launch");
     cudaEventRecord(scene->ev_stop, stream);
     scene->rendered = true;
@@ -236,6 +259,14 @@ int sol_gpu_scene_info(const SolGpuScene* scene, SolGpuSceneInfo* out) {
 int sol_gpu_scene_set_instrumented(SolGpuScene* scene, int instrumented) {
     if (!scene) return fail(SOL_GPU_ERR_INVALID_ARG, "scene must not be NULL");
     scene->instrumented = instrumented != 0;
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_scene_set_schedule(SolGpuScene* scene, int schedule) {
+    if (!scene) return fail(SOL_GPU_ERR_INVALID_ARG, "scene must not be NULL");
+    if (schedule < SOL_GPU_SCHEDULE_AUTO || schedule > SOL_GPU_SCHEDULE_SPLIT)
+        return fail(SOL_GPU_ERR_INVALID_ARG, "unknown schedule");
+    scene->schedule = schedule;
     return SOL_GPU_OK;
 }
 
@@ -389,11 +420,19 @@ int sol_gpu_adjoint(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpu
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaMemsetAsync(scene->counters, 0, sizeof(DeviceCounters), st);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
-    const int per_sm = adjoint_blocks_per_sm();
+    const uint32_t n_shared = (uint32_t)std::min<uint64_t>(scene->constants_count, kAdjointMaxSharedParams);
+    const int per_sm = adjoint_blocks_per_sm(n_shared);
     if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "adjoint occupancy query failed");
+    // Spread a pixel's samples over several lanes when the image alone would
+    // not give every resident lane a few items.
+    const uint64_t lanes = (uint64_t)per_sm * scene->num_sms * kAdjointBlock;
+    const uint64_t total = (uint64_t)((width + 7) / 8) * ((height + 3) / 4) * 32;
+    uint64_t chunks = std::min<uint64_t>(sample_count, std::max<uint64_t>(1, (4 * lanes + total - 1) / total));
+    chunks = std::max<uint64_t>(1, std::min<uint64_t>(chunks, 0xffffffffull / total));
+    const uint32_t chunk = (uint32_t)((sample_count + chunks - 1) / chunks);
     cudaEventRecord(scene->ev_start, st);
-    e = launch_adjoint(scene->view, to_camera(*camera), to_config(*config), sample_index, sample_count, width, height,
-                       dl_dfilm, grad, scene->counters, per_sm * scene->num_sms, st);
+    e = launch_adjoint(scene->view, to_camera(*camera), to_config(*config), sample_index, sample_count, chunk, width,
+                       height, dl_dfilm, grad, n_shared, scene->counters, per_sm * scene->num_sms, st);
     if (e != cudaSuccess) return cuda_fail(e, "adjoint launch");
     cudaEventRecord(scene->ev_stop, st);
     scene->rendered = true;

@@ -24,12 +24,15 @@ struct SolGpuScene {
     sol_b200::DLight* lights = nullptr;
     sol_b200::DeviceCounters* counters = nullptr;
     unsigned int* fault = nullptr;   // kFault* bits set by the kernels' self-checks
+    float* split_scratch = nullptr;  // per-sample colours of split-schedule renders
+    size_t split_floats = 0;
     float* film_tmp = nullptr;       // device film for host-film renders
     size_t film_tmp_floats = 0;
     float* film_host = nullptr;      // pinned staging for host-film renders
     size_t film_host_floats = 0;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     bool instrumented = false;
+    int schedule = SOL_GPU_SCHEDULE_AUTO;
     bool rendered = false;
     sol_b200::SceneView view{};
     SolGpuSceneInfo info{};

@@ -15,11 +15,16 @@ namespace sol_b200 {
 #ifndef SOL_MEGAKERNEL_MIN_BLOCKS
 #define SOL_MEGAKERNEL_MIN_BLOCKS 8   // 64 registers: measured fastest despite spills (latency-bound traversal)
 #endif
+#ifndef SOL_MEGAKERNEL_SHARED_STACK
+#define SOL_MEGAKERNEL_SHARED_STACK 0   // 1: first traversal-stack entries in shared memory (measured 5% slower)
+#endif
 /// Threads per block of the megakernel, and the resident blocks per SM its
 /// register allocation must allow (the compile-time occupancy target).
 constexpr int kMegakernelBlock = SOL_MEGAKERNEL_BLOCK;
 constexpr int kMegakernelMinBlocks = SOL_MEGAKERNEL_MIN_BLOCKS;
 constexpr int kTraceBlock = 128;
+/// Largest per-sample colour scratch a split-schedule render may use.
+constexpr size_t kSplitScratchMaxBytes = size_t(256) << 20;
 
 /// Resident blocks per SM of the megakernel (for sizing its persistent grid).
 int megakernel_blocks_per_sm(bool instrumented);
@@ -31,6 +36,15 @@ cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DCon
                               uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
                               float* film, DeviceCounters* counters, bool instrumented, int grid,
                               cudaStream_t stream);
+
+/// K1 in the split schedule for small images: every (pixel, sample) is its own
+/// work item; the path colours go to `scratch` (sample_count x 3 planes of
+/// width*height) and are then added into `film` in sample order.  Same result
+/// bits as launch_megakernel.  `counters` must be zeroed before the launch.
+cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, const DConfig& cfg,
+                                    uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
+                                    float* film, float* scratch, DeviceCounters* counters, bool instrumented, int grid,
+                                    cudaStream_t stream);
 
 /// K9: closest-hit or any-hit queries for a batch of rays.
 cudaError_t launch_trace(const SceneView& s, const SolGpuRay* rays, uint32_t count, bool any_hit,

@@ -9,6 +9,13 @@
 // exhausted.  One lane owns a pixel for all of its samples, which keeps the
 // per-pixel sum in SoL's sample order and the result bit-identical to the host.
 //
+// Small images (fewer pixels than a few per resident lane) use the split
+// schedule instead: a work item is one (pixel, sample), so the samples of a
+// pixel run on different lanes; each writes its path's colour (0 + colour, as
+// the per-pixel sum starts) to a scratch plane of its sample, and
+// sum_samples adds each pixel's colours in sample order, which is the same
+// sequence of additions as the per-pixel loop and gives the same bits.
+//
 // One iteration of the loop traces one closest-hit ray, shades the hit (direct
 // emission with MIS, light sample + MIS, Russian roulette, BSDF sample), then
 // traces the shadow ray of that vertex.  The light contribution is added after
@@ -16,6 +23,8 @@
 // order SoL adds them in; the random draws happen in SoL's order regardless of
 // the shadow ray's outcome.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "kernels.h"
 #include "path.cuh"
@@ -40,26 +49,35 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
     return v;
 }
 
-template <bool kCount>
+template <bool kCount, bool kSplit>
 __global__ void __launch_bounds__(kMegakernelBlock, kMegakernelMinBlocks)
 pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint32_t sample_count,
               uint32_t width, uint32_t height, float* __restrict__ film, DeviceCounters* __restrict__ ctr) {
     const uint32_t tiles_x = (width + 7u) / 8u;
     const uint32_t total = tiles_x * ((height + 3u) / 4u) * 32u;
+    // Split: `film` is the scratch of sample_count x 3 planes; items are (sample, pixel).
+    const uint32_t items = kSplit ? total * sample_count : total;
+    const uint32_t item_samples = kSplit ? 1u : sample_count;
     const size_t plane = (size_t)width * height;
     const float light_pick_prob = 1.0f / (float)s.num_lights;
 
     TraversalCounters tc{0u, 0u};
     uint32_t n_paths = 0, n_rays = 0, n_shadow = 0;
+#if SOL_MEGAKERNEL_SHARED_STACK
+    __shared__ int stack_smem[kSharedStackDepth * kMegakernelBlock];
+    SharedStack<kMegakernelBlock> stack{stack_smem + threadIdx.x};
+#else
+    LocalStack stack;
+#endif
 
     bool have_pixel = false;
-    uint32_t px = 0, py = 0, sample = 0;
+    uint32_t px = 0, py = 0, sample = 0, sample_end = 0;
     Rgb pix_sum = rgb(0.0f);
     PathState ps;
     bool done = false;
     // Self-check bounds: a lane never needs more iterations than the pixels it
     // can claim times their samples times the path length (plus one per claim).
-    const unsigned long long loop_bound = (unsigned long long)total * ((unsigned long long)sample_count + 1ull) *
+    const unsigned long long loop_bound = (unsigned long long)items * ((unsigned long long)item_samples + 1ull) *
                                           ((unsigned long long)cfg.max_path_len + 1ull) + 64ull;
     unsigned long long iterations = 0, claims = 0;
     bool alive = false;   // the lane has a path in flight
@@ -69,28 +87,38 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
         // --- make sure this lane has a live path (or stop) ------------------
         while (!alive) {
             if (++claims > loop_bound) { atomicOr(s.fault, kFaultClaimLoop); done = true; break; }
-            if (have_pixel && sample < sample_count) {
+            if (have_pixel && sample < sample_end) {
                 start_path(ps, cam, sample_index + sample, px, py, width, height);
                 ++n_paths;
                 if (cfg.max_path_len == 0) { pix_sum = pix_sum + ps.color; ++sample; continue; }
                 alive = true;
             } else {
                 if (have_pixel) {
-                    // image.h:54-60 accumulate
                     size_t i = (size_t)py * width + px;
-                    film[i] += pix_sum.r;
-                    film[i + plane] += pix_sum.g;
-                    film[i + 2 * plane] += pix_sum.b;
+                    if (kSplit) {
+                        float* f = film + (size_t)(sample_end - 1u) * 3u * plane;
+                        f[i] = pix_sum.r;
+                        f[i + plane] = pix_sum.g;
+                        f[i + 2 * plane] = pix_sum.b;
+                    } else {
+                        // image.h:54-60 accumulate
+                        film[i] += pix_sum.r;
+                        film[i + plane] += pix_sum.g;
+                        film[i + 2 * plane] += pix_sum.b;
+                    }
                     have_pixel = false;
                 }
-                uint32_t item = claim_items(&ctr->next_item);
-                if (item >= total) { done = true; break; }
-                uint32_t tile = item >> 5, l = item & 31u;
+                const uint32_t item = claim_items(&ctr->next_item);
+                if (item >= items) { done = true; break; }
+                const uint32_t k = kSplit ? item / total : 0u;
+                const uint32_t it = item - k * total;
+                uint32_t tile = it >> 5, l = it & 31u;
                 px = (tile % tiles_x) * 8u + (l & 7u);
                 py = (tile / tiles_x) * 4u + (l >> 3);
                 if (px < width && py < height) {
                     have_pixel = true;
-                    sample = 0;
+                    sample = k;
+                    sample_end = k + item_samples;
                     pix_sum = rgb(0.0f);
                 }
             }
@@ -99,7 +127,7 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
 
         // --- closest hit (path_tracer.cpp:42) ------------------------------
         float t = kFloatMax;
-        const int slot = traverse<false, kCount>(s, ps.org, ps.dir, ps.tmin, t, tc);
+        const int slot = traverse<false, kCount>(s, ps.org, ps.dir, ps.tmin, t, tc, stack);
         ++n_rays;
 
         VertexOut vo;
@@ -110,7 +138,7 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
         // --- shadow ray of this vertex (path_tracer.cpp:72-74) -------------
         if (vo.has_shadow) {
             float smax = 1.0f - cfg.ray_offset;
-            const int occ = traverse<true, kCount>(s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc);
+            const int occ = traverse<true, kCount>(s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc, stack);
             ++n_rays;
             ++n_shadow;
             if (occ < 0) ps.color = ps.color + vo.pending;
@@ -140,13 +168,25 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
     }
 }
 
+/// Adds each pixel's per-sample colours (scratch: sample_count x 3 planes) into
+/// the film in sample order, starting from 0 as the per-pixel loop does.
+__global__ void __launch_bounds__(256)
+sum_samples(const float* __restrict__ scratch, uint32_t sample_count, size_t plane, float* __restrict__ film) {
+    const size_t n = 3 * plane;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float sum = 0.0f;
+        for (uint32_t k = 0; k < sample_count; ++k) sum += scratch[(size_t)k * n + i];
+        film[i] += sum;
+    }
+}
+
 }  // namespace
 
 int megakernel_blocks_per_sm(bool instrumented) {
     int n = 0;
     cudaError_t e = instrumented
-        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pt_megakernel<true>, kMegakernelBlock, 0)
-        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pt_megakernel<false>, kMegakernelBlock, 0);
+        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pt_megakernel<true, false>, kMegakernelBlock, 0)
+        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pt_megakernel<false, false>, kMegakernelBlock, 0);
     return e == cudaSuccess ? n : -1;
 }
 
@@ -155,9 +195,25 @@ cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DCon
                               float* film, DeviceCounters* counters, bool instrumented, int grid,
                               cudaStream_t stream) {
     if (instrumented)
-        pt_megakernel<true><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, film, counters);
+        pt_megakernel<true, false><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, film, counters);
     else
-        pt_megakernel<false><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, film, counters);
+        pt_megakernel<false, false><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, film, counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, const DConfig& cfg,
+                                    uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
+                                    float* film, float* scratch, DeviceCounters* counters, bool instrumented, int grid,
+                                    cudaStream_t stream) {
+    if (instrumented)
+        pt_megakernel<true, true><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, scratch, counters);
+    else
+        pt_megakernel<false, true><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, scratch, counters);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const size_t plane = (size_t)width * height;
+    const int blocks = (int)std::min<size_t>((3 * plane + 255) / 256, 4096);
+    sum_samples<<<blocks, 256, 0, stream>>>(scratch, sample_count, plane, film);
     return cudaGetLastError();
 }
 

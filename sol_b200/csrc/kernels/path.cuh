@@ -73,25 +73,45 @@ __device__ __forceinline__ Surface make_surface(const SceneView& s, int slot, Ve
     return sf;
 }
 
+/// Observer of shade_vertex that records nothing (the forward render).  The
+/// path-replay adjoint passes an observer with the same hooks that keeps, per
+/// vertex, the quantities its reverse sweep needs; the hooks see the values the
+/// forward computes, so forward and replay cannot drift apart.
+struct NoRecord {
+    __device__ __forceinline__ void begin(const PathState&, const Surface&) {}
+    __device__ __forceinline__ void emission(const SceneView&, const DLight&, Vec3, const Surface&, Rgb, float) {}
+    __device__ __forceinline__ void before_light_sample(const DLight&, const Pcg&) {}
+    __device__ __forceinline__ void light_sample(const SceneView&, int, const DLight&, const Surface&, Vec3, Vec3, Rgb,
+                                                 Rgb, float) {}
+    __device__ __forceinline__ void survival(float, bool) {}
+    __device__ __forceinline__ void before_bounce(const SceneView&, int, const Surface&, const Pcg&) {}
+    __device__ __forceinline__ void bounce(const SceneView&, int, const Surface&, Vec3, const BsdfSample&, float) {}
+};
+
 /// One iteration of trace_path after a closest hit at (`slot`, `t`): direct
 /// emission with MIS (:48-60), light sample with MIS (:66-97, the shadow ray is
 /// returned for the caller to trace), Russian roulette (:99-108) and the BSDF
-/// bounce (:110-117), which replaces the state's ray.
+/// bounce (:110-117), which replaces the state's ray.  `rec` observes the
+/// vertex (see NoRecord).
+template <class Rec>
 __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& cfg, float light_pick_prob,
-                                             int slot, float t, PathState& ps, VertexOut& out) {
+                                             int slot, float t, PathState& ps, VertexOut& out, Rec& rec) {
     out.end = false;
     out.has_shadow = false;
     int bsdf_id, light_id;
     const Surface sf = make_surface(s, slot, ps.org, ps.dir, t, ps.tmin, &bsdf_id, &light_id);
     const Vec3 out_dir = -ps.dir;
     const uint32_t nl = s.num_lights;
+    rec.begin(ps, sf);
 
     if (light_id >= 0 && sf.front) {
         const float pdf_prev_area = ps.pdf_prev * dot(out_dir, sf.normal()) / (t * t);
         Rgb le; float pdf_from;
-        light_emission(s, s.lights[light_id], out_dir, sf.surf, &le, &pdf_from);
+        const DLight light = s.lights[light_id];
+        light_emission(s, light, out_dir, sf.surf, &le, &pdf_from);
         const float mis = ps.pdf_prev != 0.0f ? balance_heuristic(pdf_prev_area, pdf_from * light_pick_prob) : 1.0f;
         ps.color = ps.color + ps.T * le * mis;
+        rec.emission(s, light, out_dir, sf, le, mis);
     }
     if (bsdf_id < 0) { out.end = true; return; }
 
@@ -100,6 +120,7 @@ __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& 
         uint32_t li = (uint32_t)(ps.rng.next_float() * (float)nl);
         li = li < nl - 1 ? li : nl - 1;
         const DLight light = s.lights[li];
+        rec.before_light_sample(light, ps.rng);
         LightSample ls;
         if (light_sample_area(s, light, ps.rng, sf.point, &ls)) {
             Vec3 in_dir = ls.pos - sf.point;
@@ -114,23 +135,39 @@ __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& 
             const float pdf_light = ls.pdf_from * light_pick_prob;
             const float geom_term = ls.cos * inv_light_dist * inv_light_dist;
             const float mis = has_area ? balance_heuristic(pdf_light, pdf_bounce * geom_term) : 1.0f;
-            out.pending = ls.intensity * ps.T * bsdf_eval(s, bsdf_id, in_dir, sf, out_dir) *
-                          (geom_term * cos_surf * mis / pdf_light);
+            const Rgb f = bsdf_eval(s, bsdf_id, in_dir, sf, out_dir);
+            const float scale = geom_term * cos_surf * mis / pdf_light;
+            out.pending = ls.intensity * ps.T * f * scale;
             out.has_shadow = true;
+            rec.light_sample(s, bsdf_id, light, sf, in_dir, out_dir, ls.intensity, f, scale);
         }
     }
     float survival = 1.0f;
     if (ps.path_len >= cfg.min_rr_path_len) {
-        survival = clampf(luminance(ps.T), cfg.min_survival_prob, cfg.max_survival_prob);
+        const float lum = luminance(ps.T);
+        survival = clampf(lum, cfg.min_survival_prob, cfg.max_survival_prob);
+        rec.survival(survival, lum > cfg.min_survival_prob && lum < cfg.max_survival_prob);
         if (ps.rng.next_float() >= survival) { out.end = true; return; }
+    } else {
+        rec.survival(1.0f, false);
     }
+    rec.before_bounce(s, bsdf_id, sf, ps.rng);
     BsdfSample bs;
     if (!bsdf_sample(s, bsdf_id, ps.rng, sf, out_dir, &bs)) { out.end = true; return; }
-    ps.T = ps.T * (bs.color * (bs.cos / (bs.pdf * survival)));
+    const float r = bs.cos / (bs.pdf * survival);
+    ps.T = ps.T * (bs.color * r);
     ps.org = sf.point;
     ps.dir = bs.in_dir;
     ps.tmin = cfg.ray_offset;
     ps.pdf_prev = skip_nee ? 0.0f : bs.pdf;
+    rec.bounce(s, bsdf_id, sf, out_dir, bs, r);
+}
+
+/// shade_vertex for the forward render (no observer).
+__device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& cfg, float light_pick_prob,
+                                             int slot, float t, PathState& ps, VertexOut& out) {
+    NoRecord none;
+    shade_vertex(s, cfg, light_pick_prob, slot, t, ps, out, none);
 }
 
 }  // namespace sol_b200

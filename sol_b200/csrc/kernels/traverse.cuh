@@ -26,6 +26,34 @@ struct TraversalCounters {
 
 __device__ __forceinline__ float4 ldg4(const void* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 
+/// Traversal stack in local memory.
+struct LocalStack {
+    int v[kTraversalStack];
+    __device__ __forceinline__ void put(int i, int x) { v[i] = x; }
+    __device__ __forceinline__ int get(int i) const { return v[i]; }
+};
+
+/// Entries of the traversal stack kept in shared memory by SharedStack.
+constexpr int kSharedStackDepth = 16;
+
+/// Traversal stack whose first kSharedStackDepth entries live in shared memory,
+/// laid out entry-major ([entry][thread] for kThreads threads, so a warp's
+/// accesses at any mix of depths fall in distinct banks); deeper entries, which
+/// few rays reach, go to local memory.  `column` is the thread's first entry:
+/// shared_array + threadIdx.x.
+template <int kThreads>
+struct SharedStack {
+    int* column;
+    int deep[kTraversalStack - kSharedStackDepth];
+    __device__ __forceinline__ void put(int i, int x) {
+        if (i < kSharedStackDepth) column[i * kThreads] = x;
+        else deep[i - kSharedStackDepth] = x;
+    }
+    __device__ __forceinline__ int get(int i) const {
+        return i < kSharedStackDepth ? column[i * kThreads] : deep[i - kSharedStackDepth];
+    }
+};
+
 __device__ __forceinline__ Vec3 tri_vertex(float4 a) { return vec3(a.x, a.y, a.z); }
 
 /// Traverses the BVH for one ray.  For kAnyHit the first triangle hit inside
@@ -36,19 +64,18 @@ __device__ __forceinline__ Vec3 tri_vertex(float4 a) { return vec3(a.x, a.y, a.z
 /// triangle references are checked against the array sizes and the stack
 /// against its capacity; a failed check ORs a kFault* bit into `*fault` and ends
 /// the traversal (no out-of-bounds access, no unbounded loop).
-template <bool kAnyHit, bool kCount>
+template <bool kAnyHit, bool kCount, class Stack>
 __device__ __forceinline__ int traverse_bounded(const DNode* __restrict__ nodes, const DTri* __restrict__ tris,
                                         Vec3 org, Vec3 dir, float tmin, float& tmax, bool active,
                                         TraversalCounters& ctr, uint32_t num_nodes, uint32_t num_tris,
-                                        uint32_t max_steps, unsigned int* fault) {
-    int stack[kTraversalStack];
+                                        uint32_t max_steps, unsigned int* fault, Stack& stack) {
     int sp = 0;
     int hit = -1;
     uint32_t steps = 0;
     const Vec3 idir = safe_inverse(dir);
     const RayShear rs = make_shear(org, dir);
     int node = active ? 0 : kStackSentinel;
-    stack[sp++] = kStackSentinel;
+    stack.put(sp++, kStackSentinel);
 
     while (node != kStackSentinel) {
         // Descend inner nodes until a leaf (or the end) is reached.
@@ -79,7 +106,7 @@ __device__ __forceinline__ int traverse_bounded(const DNode* __restrict__ nodes,
                 int near = r.x, far = r.y;
                 if (n1 < n0) { near = r.y; far = r.x; }
                 if (sp >= kTraversalStack) { atomicOr(fault, kFaultTraversalSteps); return -1; }
-                stack[sp++] = far;
+                stack.put(sp++, far);
                 node = near;
             } else if (h0) {
                 node = r.x;
@@ -87,7 +114,7 @@ __device__ __forceinline__ int traverse_bounded(const DNode* __restrict__ nodes,
                 node = r.y;
             } else {
                 if (sp <= 0) { atomicOr(fault, kFaultTraversalSteps); return -1; }
-                node = stack[--sp];
+                node = stack.get(--sp);
             }
         }
         if (node == kStackSentinel) break;
@@ -109,17 +136,25 @@ __device__ __forceinline__ int traverse_bounded(const DNode* __restrict__ nodes,
         }
         if (kAnyHit && hit >= 0) break;
         if (sp <= 0) { atomicOr(fault, kFaultTraversalSteps); return -1; }
-        node = stack[--sp];
+        node = stack.get(--sp);
     }
     return hit;
 }
 
-/// traverse_bounded over the arrays and limits of a scene view.
+/// traverse_bounded over the arrays and limits of a scene view, with the given stack.
+template <bool kAnyHit, bool kCount, class Stack>
+__device__ __forceinline__ int traverse(const SceneView& s, Vec3 org, Vec3 dir, float tmin, float& tmax,
+                                        TraversalCounters& ctr, Stack& stack) {
+    return traverse_bounded<kAnyHit, kCount>(s.nodes, s.tris, org, dir, tmin, tmax, s.num_tris > 0, ctr, s.num_nodes,
+                                             s.num_tris, s.max_steps, s.fault, stack);
+}
+
+/// traverse with a stack in local memory.
 template <bool kAnyHit, bool kCount>
 __device__ __forceinline__ int traverse(const SceneView& s, Vec3 org, Vec3 dir, float tmin, float& tmax,
                                         TraversalCounters& ctr) {
-    return traverse_bounded<kAnyHit, kCount>(s.nodes, s.tris, org, dir, tmin, tmax, s.num_tris > 0, ctr, s.num_nodes,
-                                             s.num_tris, s.max_steps, s.fault);
+    LocalStack stack;
+    return traverse<kAnyHit, kCount>(s, org, dir, tmin, tmax, ctr, stack);
 }
 
 }  // namespace sol_b200

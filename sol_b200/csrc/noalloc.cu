@@ -116,7 +116,8 @@ extern "C" int sol_gpu_batch_forward_adjoint_noalloc(SolGpuScene* const* scenes,
         w.grad = a.grad;
         w.loss = a.loss;
         w.item_begin = (uint32_t)items;
-        items += (uint64_t)((a.view.width + 7) / 8) * ((a.view.height + 3) / 4) * 32;
+        w.group = fused_group(a.view.sample_count);
+        items += fused_items(a.view.width, a.view.height, a.view.sample_count);
         if (items > 0xffffffffull) return fail(SOL_GPU_ERR_INVALID_ARG, "batch too large");
     }
     DeviceGuard guard(device);

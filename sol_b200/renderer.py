@@ -85,6 +85,10 @@ class GpuScene:
     def set_instrumented(self, on: bool) -> None:
         capi.check(capi.lib.sol_gpu_scene_set_instrumented(self.handle, int(on)), "sol_gpu_scene_set_instrumented")
 
+    def set_schedule(self, schedule: int) -> None:
+        """capi.SCHEDULE_AUTO / SCHEDULE_PER_PIXEL / SCHEDULE_SPLIT (same film bits)."""
+        capi.check(capi.lib.sol_gpu_scene_set_schedule(self.handle, int(schedule)), "sol_gpu_scene_set_schedule")
+
     def trace(self, rays_ptr: int, count: int, any_hit: bool, hits_ptr: int, stream: int = 0) -> None:
         """Device-pointer batch query (SolGpuRay in, SolGpuHit out)."""
         capi.check(capi.lib.sol_gpu_trace(self.handle, rays_ptr, count, int(any_hit), hits_ptr, stream), "sol_gpu_trace")

@@ -235,7 +235,7 @@ def cornell_box(seed: int = 0, textured: bool = False, tex_size: int = 256, tex_
 
 
 # ---------------------------------------------------------------------------
-# Configurations 1 / 2 / 4: displaced spheres
+# Displaced-sphere scenes
 # ---------------------------------------------------------------------------
 
 def uv_sphere(bands: int = 65, segments: int = 128):
@@ -356,8 +356,57 @@ def sphere_field(num_spheres: int = 64, seed: int = 1, bands: int = 65, segments
     return mb.scene(textures=tex, bsdfs=bsdfs, lights=lights, images=images, camera=cam)
 
 
+def view_set(num_views: int = 64, seed: int = 2, box: float = 10.0, min_side: int = 64, max_side: int = 1024,
+             max_spp: int = 64):
+    """Seeded cameras into a sphere field of extent `box`: (Camera, side, spp) per view.
+
+    Per view, in draw order from Pcg(seed): square film side log-uniform in
+    [min_side, max_side], spp uniform in {1..max_spp}, eye on a ring around the
+    field (angle, radius 0.6-1.0 box, height 0.2-0.8 box), look-at point in the
+    middle of the field, field of view U[40, 70] degrees.
+    """
+    rng = Pcg(seed)
+    out = []
+    for _ in range(num_views):
+        side = int(round(math.exp(rng.uniform(math.log(min_side), math.log(max_side)))))
+        spp = 1 + min(int(rng() * max_spp), max_spp - 1)
+        ang = rng.uniform(0.0, 2.0 * math.pi)
+        r = rng.uniform(0.6, 1.0) * box
+        hgt = rng.uniform(0.2, 0.8) * box
+        eye = (0.5 * box + r * math.cos(ang), hgt, 0.5 * box + r * math.sin(ang))
+        at = (rng.uniform(0.3, 0.7) * box, rng.uniform(0.0, 0.3) * box, rng.uniform(0.3, 0.7) * box)
+        fov = rng.uniform(40.0, 70.0)
+        cam = Camera(eye=eye, dir=tuple(a - e for a, e in zip(at, eye)), up=(0.0, 1.0, 0.0), fov=fov, aspect=1.0)
+        out.append((cam, side, spp))
+    return out
+
+
+def scene_set(num_scenes: int = 32, seed: int = 4, min_tris: int = 10_000, max_tris: int = 2_000_000,
+              min_side: int = 128, max_side: int = 512, tex_size: int = 128):
+    """Independent textured sphere fields of uneven size: (Scene, side) per scene.
+
+    Per scene, in draw order from Pcg(seed): a triangle budget log-uniform in
+    [min_tris, max_tris] and a square film side log-uniform in [min_side,
+    max_side].  The budget is met with n = clamp(budget / 16384, 2, 128) spheres
+    of seg^2 triangles each (seg segments, seg/2 + 1 bands), seg the even number
+    nearest sqrt(budget / n).  Every scene has its own tex_size^2 RGB albedo
+    image (ground and half of the diffuse spheres) and its own light emission.
+    """
+    rng = Pcg(seed)
+    out = []
+    for k in range(num_scenes):
+        budget = math.exp(rng.uniform(math.log(min_tris), math.log(max_tris)))
+        side = int(round(math.exp(rng.uniform(math.log(min_side), math.log(max_side)))))
+        n = max(2, min(128, int(round(budget / 16384))))
+        seg = max(6, 2 * int(round(math.sqrt(budget / n) / 2)))
+        sizes = [(seg // 2 + 1, seg)] * n
+        out.append((sphere_field(n, seed=100 + k, textured=True, tex_size=tex_size, sphere_sizes=sizes,
+                                 aspect=1.0), side))
+    return out
+
+
 # ---------------------------------------------------------------------------
-# Named configurations
+# Named frames
 # ---------------------------------------------------------------------------
 
 CORNELL_CONFIG = Config(max_path_len=16, min_rr_path_len=3, min_survival_prob=0.05, max_survival_prob=0.75,
@@ -366,11 +415,11 @@ SPHERES_CONFIG = Config(max_path_len=8, min_rr_path_len=3, min_survival_prob=0.0
                         ray_offset=1e-4)
 
 
-def config0():
+def cornell_frame():
     """Cornell box, 256^2, 16 spp, max path length 16, RR from bounce 3."""
     return cornell_box(0), CORNELL_CONFIG, 256, 256, 16
 
 
-def config1():
+def sphere_field_frame():
     """1,048,576-triangle sphere field, 1920x1080, 64 spp, max path length 8."""
     return sphere_field(64, seed=1), SPHERES_CONFIG, 1920, 1080, 64

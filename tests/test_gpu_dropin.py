@@ -15,7 +15,7 @@ pytestmark = [pytest.mark.gpu,
 
 def test_dropin_matches_sol_pathtracer_cornell(built):
     from sol_b200 import scenes
-    scene, cfg, *_ = scenes.config0()
+    scene, cfg, *_ = scenes.cornell_frame()
     ref = oracle.RefScene(scene)
     cpu, _ = ref.render(cfg, 64, 64, 4)
     gpu = ref.render_gpu_dropin(cfg, 64, 64, 4)
@@ -40,7 +40,7 @@ def test_dropin_under_render_job(built, spf):
     with samples_per_frame < sample_count SoL re-renders some samples, and the
     drop-in reproduces that too."""
     from sol_b200 import scenes
-    scene, cfg, *_ = scenes.config0()
+    scene, cfg, *_ = scenes.cornell_frame()
     ref = oracle.RefScene(scene)
     cpu = ref.render_job(cfg, 32, 32, 4, spf)
     gpu = ref.render_gpu_dropin(cfg, 32, 32, 4, render_job=True, samples_per_frame=spf)

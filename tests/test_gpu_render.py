@@ -28,7 +28,7 @@ def gpu_render(scene, cfg, w, h, spp, index=0, film=None):
 
 def test_cornell_64_matches_oracle(built):
     from sol_b200 import scenes
-    scene, cfg, *_ = scenes.config0()
+    scene, cfg, *_ = scenes.cornell_frame()
     g = gpu_render(scene, cfg, 64, 64, 4)
     o = oracle.render(scene, cfg, 64, 64, 4)
     exact, bad = per_pixel_parity(g, o)
@@ -39,7 +39,7 @@ def test_cornell_64_matches_oracle(built):
 def test_cornell_full_config_matches_oracle(built):
     """The Cornell configuration at its full size: 256^2, 16 spp, depth 16."""
     from sol_b200 import scenes
-    scene, cfg, w, h, spp = scenes.config0()
+    scene, cfg, w, h, spp = scenes.cornell_frame()
     g = gpu_render(scene, cfg, w, h, spp)
     o = oracle.render(scene, cfg, w, h, spp)
     exact, bad = per_pixel_parity(g, o)
@@ -81,7 +81,7 @@ def test_textured_cornell_matches_oracle(built):
 def test_accumulation_and_resume(built):
     """render(0,3) + render(3,5) adds into the film like SoL; equals render(0,8) up to rounding."""
     from sol_b200 import scenes
-    scene, cfg, *_ = scenes.config0()
+    scene, cfg, *_ = scenes.cornell_frame()
     g = gpu_render(scene, cfg, 32, 32, 3, 0)
     g = gpu_render(scene, cfg, 32, 32, 5, 3, film=g)
     o = oracle.render(scene, cfg, 32, 32, 3, 0)
@@ -95,7 +95,7 @@ def test_accumulation_and_resume(built):
 @pytest.mark.parametrize("w,h", [(1, 1), (13, 7), (33, 5), (8, 4)])
 def test_odd_image_sizes(built, w, h):
     from sol_b200 import scenes
-    scene, cfg, *_ = scenes.config0()
+    scene, cfg, *_ = scenes.cornell_frame()
     g = gpu_render(scene, cfg, w, h, 2)
     o = oracle.render(scene, cfg, w, h, 2)
     exact, bad = per_pixel_parity(g, o)
@@ -176,7 +176,7 @@ def test_device_film_entry_point(built):
     import torch
     from sol_b200 import scenes
     from sol_b200.renderer import GpuPathTracer
-    scene, cfg, *_ = scenes.config0()
+    scene, cfg, *_ = scenes.cornell_frame()
     film = torch.full((3, 32, 32), 0.25, dtype=torch.float32, device="cuda")
     pt = GpuPathTracer(scene, cfg)
     stream = torch.cuda.current_stream()
@@ -188,3 +188,32 @@ def test_device_film_entry_point(built):
     st = pt.stats()
     assert st.paths == 32 * 32 * 4
     assert st.rays >= st.paths and st.shadow_rays > 0 and st.kernel_ms > 0
+
+
+@pytest.mark.parametrize("which", ["cornell", "spheres"])
+def test_schedules_agree_bit_for_bit(built, which):
+    """The per-pixel and the split schedule sum the same path colours in the same
+    order, so their films are identical; AUTO picks one of them."""
+    import torch
+    from sol_b200 import capi, scenes
+    from sol_b200.renderer import GpuPathTracer, GpuScene
+    if which == "cornell":
+        scene, cfg, w, h, spp = scenes.cornell_box(0, textured=True, tex_size=32), scenes.CORNELL_CONFIG, 96, 80, 7
+    else:
+        scene, cfg, w, h, spp = scenes.sphere_field(6, seed=3, bands=17, segments=32), scenes.SPHERES_CONFIG, 160, 90, 5
+    gs = GpuScene(scene)
+    pt = GpuPathTracer(gs, cfg)
+    stream = torch.cuda.current_stream().cuda_stream
+    films = {}
+    for sched in (capi.SCHEDULE_PER_PIXEL, capi.SCHEDULE_SPLIT, capi.SCHEDULE_AUTO):
+        gs.set_schedule(sched)
+        f = torch.full((3, h, w), 0.5, device="cuda")
+        pt.render_device(f.data_ptr(), w, h, 11, spp, stream)
+        torch.cuda.synchronize()
+        assert pt.stats().paths == w * h * spp
+        films[sched] = f
+    assert torch.equal(films[capi.SCHEDULE_PER_PIXEL], films[capi.SCHEDULE_SPLIT])
+    assert torch.equal(films[capi.SCHEDULE_PER_PIXEL], films[capi.SCHEDULE_AUTO])
+    o = oracle.render(scene, cfg, w, h, spp, sample_index=11, film=np.full((3, h, w), 0.5, np.float32))
+    exact, bad = per_pixel_parity(films[capi.SCHEDULE_SPLIT].cpu().numpy(), o)
+    assert bad == 0 and exact >= 0.999

@@ -68,7 +68,7 @@ def test_oracle_matches_sol_golden_films(built, path):
 
 @pytest.mark.skipif(not oracle.ref_available(), reason="SoL's sources are not built here")
 def test_oracle_matches_sol_pathtracer_cornell(built):
-    scene, cfg, *_ = scenes.config0()
+    scene, cfg, *_ = scenes.cornell_frame()
     a = oracle.render(scene, cfg, 64, 64, 4)
     b, _ = oracle.RefScene(scene).render(cfg, 64, 64, 4)
     exact, bad = per_pixel_parity(a, b)
@@ -78,7 +78,7 @@ def test_oracle_matches_sol_pathtracer_cornell(built):
 @pytest.mark.skipif(not oracle.ref_available(), reason="SoL's sources are not built here")
 def test_oracle_matches_sol_pathtracer_accumulation(built):
     """render(0, 2) then render(2, 3) on one film equals SoL doing the same."""
-    scene, cfg, *_ = scenes.config0()
+    scene, cfg, *_ = scenes.cornell_frame()
     a = oracle.render(scene, cfg, 16, 16, 2, 0)
     a = oracle.render(scene, cfg, 16, 16, 3, 2, film=a)
     ref = oracle.RefScene(scene)
