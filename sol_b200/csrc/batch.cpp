@@ -199,6 +199,7 @@ int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* v
     WfParams& h = b->host;
     h.capacity = (uint32_t)std::min<uint64_t>(want, std::max<uint64_t>(pixels, 32));
     h.sort_threshold = b->opts.sort_threshold;
+    h.refill_below = kWfRefillBelow;
     h.num_views = n;
     h.total_items = total_items;
     {

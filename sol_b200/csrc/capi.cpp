@@ -427,8 +427,12 @@ int sol_gpu_adjoint(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpu
     // not give every resident lane a few items.
     const uint64_t lanes = (uint64_t)per_sm * scene->num_sms * kAdjointBlock;
     const uint64_t total = (uint64_t)((width + 7) / 8) * ((height + 3) / 4) * 32;
-    uint64_t chunks = std::min<uint64_t>(sample_count, std::max<uint64_t>(1, (4 * lanes + total - 1) / total));
-    chunks = std::max<uint64_t>(1, std::min<uint64_t>(chunks, 0xffffffffull / total));
+    // One sample per item when the item count allows; otherwise enough chunks
+    // for four items per resident lane.
+    uint64_t chunks = (uint64_t)sample_count;
+    if (total * chunks > 0x7fffffffull)
+        chunks = std::min<uint64_t>(sample_count, std::max<uint64_t>(1, (4 * lanes + total - 1) / total));
+    chunks = std::max<uint64_t>(1, std::min<uint64_t>(chunks, 0x7fffffffull / total));
     const uint32_t chunk = (uint32_t)((sample_count + chunks - 1) / chunks);
     cudaEventRecord(scene->ev_start, st);
     e = launch_adjoint(scene->view, to_camera(*camera), to_config(*config), sample_index, sample_count, chunk, width,

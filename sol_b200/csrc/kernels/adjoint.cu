@@ -92,6 +92,21 @@ __device__ __forceinline__ T reduce_by_address(const void* addr, T v, bool& lead
     return sum;
 }
 
+#ifndef SOL_ADJOINT_NOINLINE
+#define SOL_ADJOINT_NOINLINE 1
+#endif
+// The adjoint kernels are large; keeping the path tracer, the sweep and the
+// texture scatter as single out-of-line copies keeps them in the instruction cache.
+#if SOL_ADJOINT_NOINLINE
+#define SOL_ADJ_OUTLINE __noinline__
+#else
+#define SOL_ADJ_OUTLINE
+#endif
+
+#ifndef SOL_ADJOINT_SAMPLE_MINOR
+#define SOL_ADJOINT_SAMPLE_MINOR 1
+#endif
+
 #ifndef SOL_ADJOINT_REDUCE_TEXELS
 #define SOL_ADJOINT_REDUCE_TEXELS 0
 #endif
@@ -119,7 +134,7 @@ __device__ __forceinline__ void atomic_add_texel(const GradSink& g, uint64_t idx
 }
 
 /// Adds `a` (d loss / d colour value) into the parameters of colour texture `tex` at `uv`.
-__device__ void scatter_color(const SceneView& s, const GradSink& grad, int tex, Vec2 uv, Rgb a) {
+__device__ SOL_ADJ_OUTLINE void scatter_color(const SceneView& s, const GradSink& grad, int tex, Vec2 uv, Rgb a) {
     if (tex < 0) return;
     const DTexture t = s.textures[tex];
     const uint64_t base = s.param_offsets[tex];
@@ -359,7 +374,7 @@ struct Recorder {
 /// Traces one path (one pixel sample) exactly as the forward render does,
 /// recording every vertex into `rec`.  Returns the number of records; `color`
 /// receives the path's colour (the same bits as the forward's).
-__device__ int trace_recorded(const SceneView& s, const DConfig& cfg, const DCamera& cam, uint64_t frame,
+__device__ SOL_ADJ_OUTLINE int trace_recorded(const SceneView& s, const DConfig& cfg, const DCamera& cam, uint64_t frame,
                               uint32_t px, uint32_t py, uint32_t width, uint32_t height, VertexRec* rec, Rgb& color,
                               uint32_t& n_rays) {
     PathState ps;
@@ -442,7 +457,7 @@ struct VertexTerms {
 /// Reverse sweep over the K records of one path with G = dL/d(path colour):
 /// carries a = dL/dT of the vertex after the current one from the last vertex
 /// to the first and adds every texture's share into `grad`.
-__device__ void sweep(const SceneView& s, const VertexRec* rec, int K, Rgb G, const GradSink& grad) {
+__device__ SOL_ADJ_OUTLINE void sweep(const SceneView& s, const VertexRec* rec, int K, Rgb G, const GradSink& grad) {
     Rgb a = rgb(0.0f);
     for (int v = K - 1; v >= 0; --v) {
         const VertexRec& R = rec[v];
@@ -505,7 +520,13 @@ prb_adjoint(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint32
         if ((int)lane() == leader) base = atomicAdd(&ctr->next_item, (uint32_t)__popc(mask));
         const uint32_t item = __shfl_sync(mask, base, leader) + __popc(mask & ((1u << lane()) - 1u));
         if (item >= items) break;
+#if SOL_ADJOINT_SAMPLE_MINOR
+        // Consecutive items are consecutive sample chunks of one pixel, so a warp
+        // replays few pixels with coherent primary rays.
+        const uint32_t it = item / chunks, c = item - it * chunks;
+#else
         const uint32_t c = item / total, it = item - c * total;
+#endif
         const uint32_t tile = it >> 5, l = it & 31u;
         const uint32_t px = (tile % tiles_x) * 8u + (l & 7u);
         const uint32_t py = (tile / tiles_x) * 4u + (l >> 3);

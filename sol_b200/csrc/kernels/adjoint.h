@@ -9,7 +9,7 @@
 namespace sol_b200 {
 
 #ifndef SOL_ADJOINT_MIN_BLOCKS
-#define SOL_ADJOINT_MIN_BLOCKS 4   // resident blocks per SM the register allocation must allow (128 registers)
+#define SOL_ADJOINT_MIN_BLOCKS 6   // resident blocks per SM the register allocation must allow (80 registers; measured fastest)
 #endif
 constexpr int kAdjointBlock = 128;
 constexpr int kAdjointMinBlocks = SOL_ADJOINT_MIN_BLOCKS;

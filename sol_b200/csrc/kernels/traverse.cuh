@@ -56,89 +56,136 @@ struct SharedStack {
 
 __device__ __forceinline__ Vec3 tri_vertex(float4 a) { return vec3(a.x, a.y, a.z); }
 
-/// Traverses the BVH for one ray.  For kAnyHit the first triangle hit inside
-/// (tmin, tmax) is returned; otherwise the closest one, with `tmax` shrunk to
-/// its distance.  Returns the triangle's position in leaf order, or -1.
-/// `active == false` lanes return -1 at once but keep the warp convergent.
-/// Self-checks: the loop runs at most `max_steps` iterations, node and
-/// triangle references are checked against the array sizes and the stack
-/// against its capacity; a failed check ORs a kFault* bit into `*fault` and ends
-/// the traversal (no out-of-bounds access, no unbounded loop).
+/// BVH traversal of one ray as a resumable state: start() sets it up, run()
+/// advances it.  For kAnyHit the first triangle hit inside (tmin, tmax) is
+/// kept; otherwise the closest one, with `tmax` shrunk to its distance.  `hit`
+/// is the triangle's position in leaf order, or -1.
+///
+/// With kYield, run() may return early, after a leaf, when fewer than
+/// `min_active` lanes of the warp are still traversing: the caller gives the
+/// lanes whose rays are done new rays and calls run() again, which continues
+/// exactly where it stopped (dynamic ray fetch; Aila & Laine, "Understanding
+/// the Efficiency of Ray Traversal on GPUs", HPG 2009).  Stopping changes
+/// nothing in the order nodes and triangles are visited, so the result is the
+/// same as an uninterrupted traversal.
+///
+/// Self-checks: at most `max_steps` steps, node and triangle references checked
+/// against the array sizes and the stack against its capacity; a failed check
+/// ORs a kFault* bit into `*fault` and ends the traversal with no hit.
+template <bool kAnyHit, bool kCount, bool kYield>
+struct Traversal {
+    Vec3 org, dir, idir;
+    RayShear rs;
+    float tmin, tmax;
+    int node, sp, hit;
+    uint32_t steps;
+
+    template <class Stack>
+    __device__ __forceinline__ void start(Vec3 o, Vec3 d, float t0, float t1, bool active, Stack& stack) {
+        org = o;
+        dir = d;
+        tmin = t0;
+        tmax = t1;
+        idir = safe_inverse(d);
+        rs = make_shear(o, d);
+        sp = 0;
+        hit = -1;
+        steps = 0;
+        node = active ? 0 : kStackSentinel;
+        stack.put(sp++, kStackSentinel);
+    }
+
+    __device__ __forceinline__ bool fail(unsigned int* fault, unsigned int bit) {
+        atomicOr(fault, bit);
+        hit = -1;
+        node = kStackSentinel;
+        return true;
+    }
+
+    /// Advances the traversal; true when it has finished.
+    template <class Stack>
+    __device__ __forceinline__ bool run(const DNode* __restrict__ nodes, const DTri* __restrict__ tris,
+                                        TraversalCounters& ctr, uint32_t num_nodes, uint32_t num_tris,
+                                        uint32_t max_steps, unsigned int* fault, Stack& stack, int min_active) {
+        while (node != kStackSentinel) {
+            // Descend inner nodes until a leaf (or the end) is reached.
+            while (node >= 0) {
+                if (++steps > max_steps) return fail(fault, kFaultTraversalSteps);
+                if ((uint32_t)node >= num_nodes) return fail(fault, kFaultNodeIndex);
+                const DNode* n = nodes + node;
+                const float4 a = ldg4(n->b0);
+                const float4 b = ldg4(n->b1);
+                const float4 c = ldg4(n->b2);
+                const int4 r = __ldg(reinterpret_cast<const int4*>(n->ref));
+                if (kCount) ctr.nodes++;
+                // (bound - org) * (1/dir): two correctly rounded operations per plane, so the
+                // widened exit distance stays conservative even for grazing rays (the
+                // product-with-offset form loses |org / dir| ulps to cancellation).
+                float t0lx = (a.x - org.x) * idir.x, t0hx = (a.y - org.x) * idir.x;
+                float t0ly = (a.z - org.y) * idir.y, t0hy = (a.w - org.y) * idir.y;
+                float t0lz = (c.x - org.z) * idir.z, t0hz = (c.y - org.z) * idir.z;
+                float t1lx = (b.x - org.x) * idir.x, t1hx = (b.y - org.x) * idir.x;
+                float t1ly = (b.z - org.y) * idir.y, t1hy = (b.w - org.y) * idir.y;
+                float t1lz = (c.z - org.z) * idir.z, t1hz = (c.w - org.z) * idir.z;
+                float n0 = fmaxf(fmaxf(fminf(t0lx, t0hx), fminf(t0ly, t0hy)), fmaxf(fminf(t0lz, t0hz), tmin));
+                float f0 = fminf(fminf(fmaxf(t0lx, t0hx), fmaxf(t0ly, t0hy)), fminf(fmaxf(t0lz, t0hz), tmax)) * kSlabWiden;
+                float n1 = fmaxf(fmaxf(fminf(t1lx, t1hx), fminf(t1ly, t1hy)), fmaxf(fminf(t1lz, t1hz), tmin));
+                float f1 = fminf(fminf(fmaxf(t1lx, t1hx), fmaxf(t1ly, t1hy)), fminf(fmaxf(t1lz, t1hz), tmax)) * kSlabWiden;
+                const bool h0 = n0 <= f0, h1 = n1 <= f1;
+                if (h0 && h1) {
+                    int near = r.x, far = r.y;
+                    if (n1 < n0) { near = r.y; far = r.x; }
+                    if (sp >= kTraversalStack) return fail(fault, kFaultTraversalSteps);
+                    stack.put(sp++, far);
+                    node = near;
+                } else if (h0) {
+                    node = r.x;
+                } else if (h1) {
+                    node = r.y;
+                } else {
+                    if (sp <= 0) return fail(fault, kFaultTraversalSteps);
+                    node = stack.get(--sp);
+                }
+            }
+            if (node == kStackSentinel) break;
+            // Leaf: ~node = (first << 3) | (count - 1)
+            const uint32_t v = ~(uint32_t)node;
+            const uint32_t first = v >> 3, count = (v & 7u) + 1u;
+            if (first + count > num_tris) return fail(fault, kFaultTriIndex);
+            if (++steps > max_steps) return fail(fault, kFaultTraversalSteps);
+            for (uint32_t i = first; i < first + count; ++i) {
+                const DTri* tp = tris + i;
+                const float4 p0 = ldg4(tp->v0), p1 = ldg4(tp->v1), p2 = ldg4(tp->v2);
+                if (kCount) ctr.tris++;
+                float t, u, w;
+                if (intersect_triangle(rs, tri_vertex(p0), tri_vertex(p1), tri_vertex(p2), tmin, tmax, &t, &u, &w)) {
+                    hit = (int)i;
+                    tmax = t;
+                    if (kAnyHit) break;
+                }
+            }
+            if (kAnyHit && hit >= 0) return true;
+            if (sp <= 0) return fail(fault, kFaultTraversalSteps);
+            node = stack.get(--sp);
+            if (kYield && node != kStackSentinel && __popc(__activemask()) < min_active) return false;
+        }
+        return true;
+    }
+};
+
+/// Traverses the BVH for one ray to completion (see Traversal).  Returns the
+/// hit triangle's position in leaf order, or -1; `tmax` becomes the hit
+/// distance.  `active == false` lanes return -1 at once.
 template <bool kAnyHit, bool kCount, class Stack>
 __device__ __forceinline__ int traverse_bounded(const DNode* __restrict__ nodes, const DTri* __restrict__ tris,
                                         Vec3 org, Vec3 dir, float tmin, float& tmax, bool active,
                                         TraversalCounters& ctr, uint32_t num_nodes, uint32_t num_tris,
                                         uint32_t max_steps, unsigned int* fault, Stack& stack) {
-    int sp = 0;
-    int hit = -1;
-    uint32_t steps = 0;
-    const Vec3 idir = safe_inverse(dir);
-    const RayShear rs = make_shear(org, dir);
-    int node = active ? 0 : kStackSentinel;
-    stack.put(sp++, kStackSentinel);
-
-    while (node != kStackSentinel) {
-        // Descend inner nodes until a leaf (or the end) is reached.
-        while (node >= 0) {
-            if (++steps > max_steps) { atomicOr(fault, kFaultTraversalSteps); return -1; }
-            if ((uint32_t)node >= num_nodes) { atomicOr(fault, kFaultNodeIndex); return -1; }
-            const DNode* n = nodes + node;
-            const float4 a = ldg4(n->b0);
-            const float4 b = ldg4(n->b1);
-            const float4 c = ldg4(n->b2);
-            const int4 r = __ldg(reinterpret_cast<const int4*>(n->ref));
-            if (kCount) ctr.nodes++;
-            // (bound - org) * (1/dir): two correctly rounded operations per plane, so the
-            // widened exit distance stays conservative even for grazing rays (the
-            // product-with-offset form loses |org / dir| ulps to cancellation).
-            float t0lx = (a.x - org.x) * idir.x, t0hx = (a.y - org.x) * idir.x;
-            float t0ly = (a.z - org.y) * idir.y, t0hy = (a.w - org.y) * idir.y;
-            float t0lz = (c.x - org.z) * idir.z, t0hz = (c.y - org.z) * idir.z;
-            float t1lx = (b.x - org.x) * idir.x, t1hx = (b.y - org.x) * idir.x;
-            float t1ly = (b.z - org.y) * idir.y, t1hy = (b.w - org.y) * idir.y;
-            float t1lz = (c.z - org.z) * idir.z, t1hz = (c.w - org.z) * idir.z;
-            float n0 = fmaxf(fmaxf(fminf(t0lx, t0hx), fminf(t0ly, t0hy)), fmaxf(fminf(t0lz, t0hz), tmin));
-            float f0 = fminf(fminf(fmaxf(t0lx, t0hx), fmaxf(t0ly, t0hy)), fminf(fmaxf(t0lz, t0hz), tmax)) * kSlabWiden;
-            float n1 = fmaxf(fmaxf(fminf(t1lx, t1hx), fminf(t1ly, t1hy)), fmaxf(fminf(t1lz, t1hz), tmin));
-            float f1 = fminf(fminf(fmaxf(t1lx, t1hx), fmaxf(t1ly, t1hy)), fminf(fmaxf(t1lz, t1hz), tmax)) * kSlabWiden;
-            const bool h0 = n0 <= f0, h1 = n1 <= f1;
-            if (h0 && h1) {
-                int near = r.x, far = r.y;
-                if (n1 < n0) { near = r.y; far = r.x; }
-                if (sp >= kTraversalStack) { atomicOr(fault, kFaultTraversalSteps); return -1; }
-                stack.put(sp++, far);
-                node = near;
-            } else if (h0) {
-                node = r.x;
-            } else if (h1) {
-                node = r.y;
-            } else {
-                if (sp <= 0) { atomicOr(fault, kFaultTraversalSteps); return -1; }
-                node = stack.get(--sp);
-            }
-        }
-        if (node == kStackSentinel) break;
-        // Leaf: ~node = (first << 3) | (count - 1)
-        const uint32_t v = ~(uint32_t)node;
-        const uint32_t first = v >> 3, count = (v & 7u) + 1u;
-        if (first + count > num_tris) { atomicOr(fault, kFaultTriIndex); return -1; }
-        if (++steps > max_steps) { atomicOr(fault, kFaultTraversalSteps); return -1; }
-        for (uint32_t i = first; i < first + count; ++i) {
-            const DTri* tp = tris + i;
-            const float4 p0 = ldg4(tp->v0), p1 = ldg4(tp->v1), p2 = ldg4(tp->v2);
-            if (kCount) ctr.tris++;
-            float t, u, w;
-            if (intersect_triangle(rs, tri_vertex(p0), tri_vertex(p1), tri_vertex(p2), tmin, tmax, &t, &u, &w)) {
-                hit = (int)i;
-                tmax = t;
-                if (kAnyHit) break;
-            }
-        }
-        if (kAnyHit && hit >= 0) break;
-        if (sp <= 0) { atomicOr(fault, kFaultTraversalSteps); return -1; }
-        node = stack.get(--sp);
-    }
-    return hit;
+    Traversal<kAnyHit, kCount, false> tr;
+    tr.start(org, dir, tmin, tmax, active, stack);
+    tr.run(nodes, tris, ctr, num_nodes, num_tris, max_steps, fault, stack, 0);
+    tmax = tr.tmax;
+    return tr.hit;
 }
 
 /// traverse_bounded over the arrays and limits of a scene view, with the given stack.

@@ -9,6 +9,9 @@
 //                  starts its pixel's next sample (camera ray).
 //   extend   (K3): closest-hit traversal of the queued rays; hits are binned by
 //                  the BSDF kind of the hit triangle (K6), misses end the path.
+//                  Persistent warps fetch rays lane by lane: when fewer than
+//                  `refill_below` lanes of a warp are still traversing, the warp
+//                  pauses, gives its idle lanes new rays and resumes.
 //   shade    (K5): SoL's per-vertex step (emission MIS, light sample, Russian
 //                  roulette, BSDF bounce) over the bins, kind by kind.
 //   shadow   (K4): any-hit traversal of the light samples' shadow rays.
@@ -114,6 +117,7 @@ __global__ void __launch_bounds__(256) wf_init(const WfParams* __restrict__ Pp) 
         c->extend[0] = c->extend[1] = 0;
         for (int b = 0; b < kWfBins; ++b) c->bins[b] = 0;
         c->shadow = 0;
+        c->fetch_extend = c->fetch_shadow = 0;
         c->next_item = 0;
         c->iter = 0;
         c->paths = c->rays = c->shadow_rays = 0;
@@ -187,34 +191,81 @@ __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ 
     if (lane_id() == 0 && paths) atomicAdd(&ctr->paths, paths);
 }
 
+/// Persistent traversal of a ray queue with dynamic ray fetch: every lane keeps
+/// one ray; at the top of each round the warp claims queue entries for its idle
+/// lanes with one atomic, then traverses until the ray is done or the warp has
+/// fewer than `refill_below` busy lanes.  `fetch(i, tr, stack, slot, sv)` starts
+/// queue entry i; `finish(slot, tr)` consumes a finished ray.
+template <bool kAnyHit, class Fetch, class Finish>
+__device__ __forceinline__ void trace_queue(uint32_t n, uint32_t* fetch_counter, int refill_below, Fetch fetch,
+                                            Finish finish, unsigned long long& rays) {
+    Traversal<kAnyHit, false, true> tr;
+    LocalStack stack;
+    const SceneView* sv = nullptr;
+    uint32_t slot = 0;
+    bool has = false;
+    bool more = true;   // warp-uniform: the queue may still hold entries
+    TraversalCounters tc{0u, 0u};
+    while (true) {
+        __syncwarp();
+        if (more) {
+            const unsigned want = __ballot_sync(0xffffffffu, !has);
+            if (want) {
+                const int leader = __ffs(want) - 1;
+                uint32_t base = 0;
+                if ((int)lane_id() == leader) base = atomicAdd(fetch_counter, (uint32_t)__popc(want));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (base + (uint32_t)__popc(want) >= n) more = false;
+                if (!has) {
+                    const uint32_t i = base + __popc(want & ((1u << lane_id()) - 1u));
+                    if (i < n) {
+                        fetch(i, tr, stack, slot, sv);
+                        has = true;
+                        ++rays;
+                    }
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, has)) break;
+        // Once the queue is drained there is nothing to refill: run to the end.
+        if (has && tr.run(sv->nodes, sv->tris, tc, sv->num_nodes, sv->num_tris, sv->max_steps, sv->fault, stack,
+                          more ? refill_below : 0)) {
+            finish(slot, tr);
+            has = false;
+        }
+    }
+}
+
 /// K3: closest hit for every queued ray; hits binned by BSDF kind (K6), misses end.
-__global__ void __launch_bounds__(256) wf_extend(const WfParams* __restrict__ Pp) {
+__global__ void __launch_bounds__(256, kWfTraceMinBlocks) wf_extend(const WfParams* __restrict__ Pp) {
     const WfParams& P = *Pp;
     WfCounters* ctr = P.ctr;
     const uint32_t p = ctr->iter & 1u;
     const uint32_t n = ctr->extend[p];
     const bool sort = n >= P.sort_threshold;
     unsigned long long rays = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = P.q_extend[p][i];
+    auto fetch = [&](uint32_t i, Traversal<false, false, true>& tr, LocalStack& stack, uint32_t& slot,
+                     const SceneView*& sv) {
+        slot = P.q_extend[p][i];
         const float4 o = P.ray_o[slot], d = P.ray_d[slot];
-        const SceneView& sv = P.scenes[P.views[P.pix[slot].x].scene];
-        float t = kFloatMax;
-        TraversalCounters tc{0u, 0u};
-        const int hit = traverse<false, false>(sv, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, t, tc);
-        ++rays;
-        if (hit < 0) {
+        sv = &P.scenes[P.views[P.pix[slot].x].scene];
+        tr.start(vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, kFloatMax, sv->num_tris > 0, stack);
+    };
+    auto finish = [&](uint32_t slot, const Traversal<false, false, true>& tr) {
+        if (tr.hit < 0) {
             P.q_regen[p ^ 1u][append(&ctr->regen[p ^ 1u])] = slot;
         } else {
-            P.hit[slot] = make_float2(__int_as_float(hit), t);
+            P.hit[slot] = make_float2(__int_as_float(tr.hit), tr.tmax);
             int kind = kWfBins - 1;
             if (sort) {
-                const int b = __ldg(&sv.tris[hit].bsdf);
+                const SceneView& sv = P.scenes[P.views[P.pix[slot].x].scene];
+                const int b = __ldg(&sv.tris[tr.hit].bsdf);
                 kind = b < 0 ? kWfBins - 1 : sv.bsdfs[b].kind;
             }
             P.q_bins[(size_t)kind * P.capacity + append_keyed(ctr->bins, kind)] = slot;
         }
-    }
+    };
+    trace_queue<false>(n, &ctr->fetch_extend, P.refill_below, fetch, finish, rays);
     rays = warp_sum(rays);
     if (lane_id() == 0 && rays) atomicAdd(&ctr->rays, rays);
 }
@@ -258,28 +309,30 @@ __global__ void __launch_bounds__(256) wf_shade(const WfParams* __restrict__ Pp)
 }
 
 /// K4: shadow rays; the light sample's contribution is added when unoccluded.
-__global__ void __launch_bounds__(256) wf_shadow(const WfParams* __restrict__ Pp) {
+__global__ void __launch_bounds__(256, kWfTraceMinBlocks) wf_shadow(const WfParams* __restrict__ Pp) {
     const WfParams& P = *Pp;
     WfCounters* ctr = P.ctr;
     const uint32_t p = ctr->iter & 1u;
     const uint32_t n = ctr->shadow;
     const float offset = P.cfg.ray_offset;
     unsigned long long rays = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = P.q_shadow[i];
-        const float4 o = P.sh_o[slot], d = P.sh_d[slot], pend = P.pending[slot];
-        const SceneView& sv = P.scenes[P.views[P.pix[slot].x].scene];
-        float smax = 1.0f - offset;
-        TraversalCounters tc{0u, 0u};
-        const int occ = traverse<true, false>(sv, vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), offset, smax, tc);
-        ++rays;
-        if (occ < 0) {
+    auto fetch = [&](uint32_t i, Traversal<true, false, true>& tr, LocalStack& stack, uint32_t& slot,
+                     const SceneView*& sv) {
+        slot = P.q_shadow[i];
+        const float4 o = P.sh_o[slot], d = P.sh_d[slot];
+        sv = &P.scenes[P.views[P.pix[slot].x].scene];
+        tr.start(vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), offset, 1.0f - offset, sv->num_tris > 0, stack);
+    };
+    auto finish = [&](uint32_t slot, const Traversal<true, false, true>& tr) {
+        const float4 pend = P.pending[slot];
+        if (tr.hit < 0) {
             const float4 c = P.color[slot];
             P.color[slot] = make_float4(c.x + pend.x, c.y + pend.y, c.z + pend.z, 0.0f);
         }
         if (pend.w != 0.0f) P.q_regen[p ^ 1u][append(&ctr->regen[p ^ 1u])] = slot;
         else P.q_extend[p ^ 1u][append(&ctr->extend[p ^ 1u])] = slot;
-    }
+    };
+    trace_queue<true>(n, &ctr->fetch_shadow, P.refill_below, fetch, finish, rays);
     rays = warp_sum(rays);
     if (lane_id() == 0 && rays) { atomicAdd(&ctr->rays, rays); atomicAdd(&ctr->shadow_rays, rays); }
 }
@@ -293,6 +346,7 @@ __global__ void wf_advance(const WfParams* __restrict__ Pp, cudaGraphConditional
     c->regen[p] = 0;
     for (int b = 0; b < kWfBins; ++b) c->bins[b] = 0;
     c->shadow = 0;
+    c->fetch_extend = c->fetch_shadow = 0;
     c->iter += 1;
     bool more = c->extend[p ^ 1u] + c->regen[p ^ 1u] > 0;
     if (more && c->iter >= P.max_iterations) { c->error |= kFaultPathLoop; more = false; }

@@ -12,6 +12,20 @@ namespace sol_b200 {
 /// (and for everything when binning is off).
 constexpr int kWfBins = 6;
 
+#ifndef SOL_WF_REFILL_BELOW
+#define SOL_WF_REFILL_BELOW 20
+#endif
+/// A traversal warp pauses to give idle lanes new rays once fewer than this
+/// many of its 32 lanes are still traversing (32 + 1 would refill after every
+/// leaf, 1 never before the warp drains).
+constexpr int kWfRefillBelow = SOL_WF_REFILL_BELOW;
+
+#ifndef SOL_WF_TRACE_MIN_BLOCKS
+#define SOL_WF_TRACE_MIN_BLOCKS 1
+#endif
+/// Resident 256-thread blocks per SM the traversal stages' registers must allow.
+constexpr int kWfTraceMinBlocks = SOL_WF_TRACE_MIN_BLOCKS;
+
 /// One view of a batch: a constructed camera, its film and sample range.
 struct WfView {
     float eye[3], dir[3], right[3], up[3];
@@ -29,6 +43,8 @@ struct WfCounters {
     uint32_t regen[2];
     uint32_t bins[kWfBins];
     uint32_t shadow;
+    uint32_t fetch_extend;   // rays taken from the extend / shadow queue by the traversal stages
+    uint32_t fetch_shadow;
     uint32_t next_item;
     uint32_t iter;
     uint32_t more;
@@ -44,6 +60,7 @@ struct WfParams {
     uint32_t num_views;
     uint32_t total_items;
     unsigned long long max_iterations;   // self-check bound on bounce-loop iterations
+    int refill_below;        // a traversal warp refills its idle lanes when fewer than this many are busy
     DConfig cfg;
     const WfView* views;
     const SceneView* scenes;
