@@ -114,28 +114,32 @@ def run_views(args, ClockSampler, load_peaks):
         for (cam, s, p), pt, f in zip(views, tracers, films):
             pt.render_device(f.data_ptr(), s, s, i * 64, p, sp)
 
-    br = BatchRenderer([gs])
+    from sol_b200 import capi
+    br = BatchRenderer([gs], schedule=capi.BATCH_AUTO)        # autotuned: wavefront or multi-view megakernel
+    br_wf = BatchRenderer([gs], schedule=capi.BATCH_WAVEFRONT)
 
-    def varr(i, fl=None):
+    def varr(i, fl=None, r=None):
         fl = fl or films
-        return br.views([(0, cam, s, s, i * 64, p, f.data_ptr()) for (cam, s, p), f in zip(views, fl)])
+        return (r or br).views([(0, cam, s, s, i * 64, p, f.data_ptr()) for (cam, s, p), f in zip(views, fl)])
 
     t0 = time.perf_counter()
     opts = br.autotune(cfg, varr(0))
     tune_s = time.perf_counter() - t0
-    arrays = {}
+    opts_wf = br_wf.autotune(cfg, varr(0, r=br_wf))
+    arrays = {i: varr(i) for i in range(args.warmup + args.steps)}
+    arrays_wf = {i: varr(i, r=br_wf) for i in range(args.warmup + args.steps)}
 
     def batched(i):
-        if i not in arrays:
-            arrays[i] = varr(i)
         br.render(cfg, arrays[i], sp)
 
-    for i in range(args.warmup + args.steps):
-        arrays[i] = varr(i)
+    def wavefront(i):
+        br_wf.render(cfg, arrays_wf[i], sp)
+
     with ClockSampler(torch.cuda.current_device()) as clocks:
         plain_ms = _timed(torch, flush, stream, plain, args.steps, args.warmup)
         batch_ms = _timed(torch, flush, stream, batched, args.steps, args.warmup)
-    plain_s, batch_s = sum(plain_ms) / 1000.0, sum(batch_ms) / 1000.0
+        wf_ms = _timed(torch, flush, stream, wavefront, args.steps, args.warmup)
+    plain_s, batch_s, wf_s = sum(plain_ms) / 1000.0, sum(batch_ms) / 1000.0, sum(wf_ms) / 1000.0
 
     # Same films from both schedules (one fresh render each).
     fa = [torch.zeros_like(f) for f in films]
@@ -143,8 +147,10 @@ def run_views(args, ClockSampler, load_peaks):
     for (cam, s, p), pt, f in zip(views, tracers, fa):
         pt.render_device(f.data_ptr(), s, s, 0, p, sp)
     br.render(cfg, varr(0, fb), sp)
+    fc = [torch.zeros_like(f) for f in films]
+    br_wf.render(cfg, varr(0, fc, br_wf), sp)
     torch.cuda.synchronize()
-    identical = all(torch.equal(a, b) for a, b in zip(fa, fb))
+    identical = all(torch.equal(a, b) and torch.equal(a, c) for a, b, c in zip(fa, fb, fc))
 
     # RMSE of each schedule's images against a 256-spp render of every view.
     gt_spp = 256
@@ -182,22 +188,27 @@ def run_views(args, ClockSampler, load_peaks):
     peak, src = load_peaks()
     achieved = alg / (batch_s / args.steps) / 1e9
     import ctypes
-    from sol_b200 import capi
     cfgd = {"workload": f"{len(views)} uneven views (side log-U[64,{views and max(s for _, s, _ in views)}], "
-                        f"1-64 spp) of a {info.num_triangles}-triangle sphere field, batched wavefront (one call) "
-                        f"vs {len(views)} plain megakernel launches",
+                        f"1-64 spp) of a {info.num_triangles}-triangle sphere field, batched (one call, autotuned "
+                        f"schedule) vs {len(views)} plain megakernel launches",
             "triangles": info.num_triangles, "views": len(views), "paths_per_step": int(paths),
             "pixels": int(sum(s * s for _, s, _ in views)), "max_path_len": cfg.max_path_len,
             "l2": "flushed between steps (256 MiB write); scene larger than L2",
-            "batch_options": {"capacity": opts.capacity, "block_size": opts.block_size,
-                              "sort_threshold": opts.sort_threshold}, "small": bool(small)}
+            "batch_options": {"schedule": ["wavefront", "megakernel", "auto"][opts.schedule],
+                              "capacity": opts.capacity, "block_size": opts.block_size,
+                              "sort_threshold": opts.sort_threshold},
+            "wavefront_options": {"capacity": opts_wf.capacity, "block_size": opts_wf.block_size,
+                                  "sort_threshold": opts_wf.sort_threshold}, "small": bool(small)}
     return _common(
         args, METRIC, paths * args.steps / batch_s / 1e6, METRIC, 1000.0 * batch_s / args.steps, True, cfgd,
         clocks.summary(), args.steps,
-        launch_note="per batched step: one call (stage kernels in a CUDA graph); per plain step: one launch per view",
+        launch_note="per batched step: one call (one megakernel launch, or the wavefront's stage kernels in a CUDA "
+                    "graph); per plain step: one launch per view",
         plain={"value": paths * args.steps / plain_s / 1e6, "unit": METRIC,
                "ms_per_step": 1000.0 * plain_s / args.steps, "launches_per_step": len(views)},
         speedup_vs_plain=plain_s / batch_s,
+        wavefront={"value": paths * args.steps / wf_s / 1e6, "unit": METRIC, "ms_per_step": 1000.0 * wf_s / args.steps,
+                   "speedup_vs_plain": plain_s / wf_s},
         equal_rmse={"films_bit_identical": identical, "reference": f"{gt_spp}-spp megakernel render per view",
                     "rmse_plain_mean": float(np.mean(rmse_a)), "rmse_batched_mean": float(np.mean(rmse_b))},
         roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -357,9 +368,16 @@ def run_scenes(args, ClockSampler, load_peaks):
                          for k, s in enumerate(sides)])
     opts = br.autotune(cfg, varr(0))
     arrays = {i: varr(i) for i in range(args.warmup + args.steps)}
+    from sol_b200 import capi
+    br_mk = BatchRenderer(gss, schedule=capi.BATCH_MEGAKERNEL)
+    arrays_mk = {i: br_mk.views([(k, made[k][0].camera, s, s, i * SPP, SPP, films[k].data_ptr())
+                                 for k, s in enumerate(sides)]) for i in range(args.warmup + args.steps)}
 
     def batched(i):
         br.render(cfg, arrays[i], sp)
+
+    def batched_mk(i):
+        br_mk.render(cfg, arrays_mk[i], sp)
 
     def plain(i):
         for pt, s, f in zip(tracers, sides, films):
@@ -368,9 +386,10 @@ def run_scenes(args, ClockSampler, load_peaks):
     with ClockSampler(torch.cuda.current_device()) as clocks:
         x_ms = _timed(torch, flush, stream, fused, args.steps, args.warmup)
         b_ms = _timed(torch, flush, stream, batched, args.steps, args.warmup)
+        m_ms = _timed(torch, flush, stream, batched_mk, args.steps, args.warmup)
         p_ms = _timed(torch, flush, stream, plain, args.steps, args.warmup)
-    fus, bat, pla = np.mean(x_ms), np.mean(b_ms), np.mean(p_ms)
-    fwd = min(bat, pla)
+    fus, bat, bmk, pla = np.mean(x_ms), np.mean(b_ms), np.mean(m_ms), np.mean(p_ms)
+    fwd = min(bat, bmk, pla)
 
     # Per-scene gradient check: 16 parameters against central differences of the forward.
     for f in films:
@@ -406,7 +425,7 @@ def run_scenes(args, ClockSampler, load_peaks):
     return _common(
         args, METRIC, paths / fus / 1e3, METRIC, fus, True, cfgd, clocks.summary(), args.steps,
         note="value: paths rendered and differentiated per second by the fused launch",
-        forward_ms={"batched_wavefront": bat, "plain_megakernel_launches": pla},
+        forward_ms={"batched_wavefront": bat, "batched_megakernel": bmk, "plain_megakernel_launches": pla},
         fused_ms=fus, fused_over_forward=fus / fwd, adjoint_over_forward=(fus - fwd) / fwd,
         gradient_check={"params_per_scene": 16, "eps": EPS, "rel_err_max": float(np.max(errs)),
                         "rel_err_median": float(np.median(errs)),

@@ -291,7 +291,17 @@ typedef struct SolGpuBatchOptions {
     uint32_t sort_threshold;  /* bin hits by BSDF kind when at least this many rays are queued
                                  (0 = always; 0xffffffff = never) */
     int32_t host_loop;        /* 1: bounce loop driven from the host instead of the graph */
+    int32_t schedule;         /* SOL_GPU_BATCH_WAVEFRONT, _MEGAKERNEL or _AUTO (below) */
 } SolGpuBatchOptions;
+
+/* Batch schedules.  WAVEFRONT: the queue-based wavefront (capacity, block size
+ * and sort threshold apply).  MEGAKERNEL: one persistent megakernel launch over
+ * all views, lanes claiming pixels of any view.  AUTO: sol_gpu_batch_autotune
+ * times both and adopts the faster; before that, AUTO renders as WAVEFRONT.
+ * Every schedule gives each film the bits sol_gpu_render_device gives it. */
+#define SOL_GPU_BATCH_WAVEFRONT  0
+#define SOL_GPU_BATCH_MEGAKERNEL 1
+#define SOL_GPU_BATCH_AUTO       2
 
 typedef struct SolGpuBatch SolGpuBatch;
 
@@ -309,9 +319,10 @@ int sol_gpu_batch_render(SolGpuBatch* batch, const SolGpuConfig* config, const S
 /* Counters and device time of the last batch render (waits for it). */
 int sol_gpu_batch_stats(SolGpuBatch* batch, SolGpuRenderStats* out);
 
-/* Times candidate options (capacity, block size, binning threshold) on one
- * sample per pixel of the given views, rendered into scratch films, adopts the
- * fastest and returns it in `chosen`.  With `cache_path` set, a previous
+/* Times candidate options (capacity, block size, binning threshold; with
+ * schedule AUTO also the megakernel schedule) on one sample per pixel of the
+ * given views, rendered into scratch films, adopts the fastest and returns it
+ * in `chosen`.  With `cache_path` set, a previous
  * choice for the same device and batch shape is read from that file instead,
  * and new choices are appended to it. */
 int sol_gpu_batch_autotune(SolGpuBatch* batch, const SolGpuConfig* config, const SolGpuView* views,

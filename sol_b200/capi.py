@@ -24,6 +24,7 @@ ERR_BAD_INDEX = -6
 ERR_UNSUPPORTED = -7
 ERR_CANCELLED = -8
 SCHEDULE_AUTO, SCHEDULE_PER_PIXEL, SCHEDULE_SPLIT = 0, 1, 2
+BATCH_WAVEFRONT, BATCH_MEGAKERNEL, BATCH_AUTO = 0, 1, 2
 
 BSDF_DIFFUSE, BSDF_PHONG, BSDF_MIRROR, BSDF_GLASS, BSDF_INTERP = range(5)
 TEX_CONSTANT, TEX_CONSTANT_COLOR, TEX_IMAGE = range(3)
@@ -108,7 +109,7 @@ class SolGpuAdjointView(C.Structure):
 
 class SolGpuBatchOptions(C.Structure):
     _fields_ = [("capacity", C.c_uint32), ("block_size", C.c_uint32), ("sort_threshold", C.c_uint32),
-                ("host_loop", C.c_int32)]
+                ("host_loop", C.c_int32), ("schedule", C.c_int32)]
 
 
 ScenePtr = C.c_void_p

@@ -14,6 +14,7 @@
 #include "../../include/sol_gpu.h"
 #include "host/handles.h"
 #include "kernels/adjoint.h"
+#include "kernels/kernels.h"
 #include "kernels/wavefront.h"
 
 using namespace sol_b200;
@@ -33,7 +34,9 @@ struct SolGpuBatch {
     size_t views_cap = 0;
     AdjView* d_adj_views = nullptr;
     size_t adj_views_cap = 0;
-    DeviceCounters* d_fused_ctr = nullptr;
+    DeviceCounters* d_dc = nullptr;   // counters of the megakernel-type launches
+    float* scratch = nullptr;         // per-sample colours of split views (megakernel schedule)
+    uint64_t scratch_floats = 0;
     WfLaunch launch{};
     int launch_block = 0;
     cudaGraph_t graph = nullptr;
@@ -42,7 +45,7 @@ struct SolGpuBatch {
     WfCounters* h_ctr = nullptr;      // pinned, for the host-driven loop
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     bool rendered = false;
-    bool last_fused = false;          // the last launch was sol_gpu_batch_forward_adjoint
+    bool last_dc = false;             // the last launch counted into d_dc (megakernel schedules)
 };
 
 namespace {
@@ -144,10 +147,45 @@ int build_graph(SolGpuBatch* b) {
     return SOL_GPU_OK;
 }
 
+/// Largest per-sample colour scratch the multi-view megakernel may use for
+/// its split views; views beyond it run per pixel.
+constexpr uint64_t kViewsScratchMaxBytes = uint64_t(4) << 30;
+
+/// Builds and uploads the view table.  For the megakernel schedule, views with
+/// fewer pixels than twice the resident lanes are split ((sample, pixel) work
+/// items, colours in scratch), as sol_gpu_render_device's AUTO schedule would
+/// split them; `sum_floats` receives the size of their sum pass.
 int upload_views(SolGpuBatch* b, const SolGpuView* views, uint32_t n, uint32_t* total_items, uint64_t* pixels,
-                 cudaStream_t stream) {
+                 cudaStream_t stream, bool megakernel = false, uint64_t* sum_floats = nullptr) {
     std::vector<WfView> v(n);
     uint64_t items = 0, px = 0;
+    uint64_t lanes = 0;
+    if (megakernel) {
+        const int per_sm = megakernel_views_blocks_per_sm();
+        if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
+        lanes = (uint64_t)per_sm * b->num_sms * kMegakernelBlock;
+    }
+    std::vector<uint64_t> scratch_at(n, 0);
+    uint64_t scratch_floats = 0, sum_at = 0;
+    if (megakernel) {
+        for (uint32_t i = 0; i < n; ++i) {
+            const SolGpuView& s = views[i];
+            const uint64_t plane = (uint64_t)s.width * s.height;
+            const uint64_t need = 3 * plane * s.sample_count;
+            if (s.sample_count > 1 && plane < 2 * lanes && (scratch_floats + need) * sizeof(float) <= kViewsScratchMaxBytes) {
+                scratch_at[i] = scratch_floats + 1;   // + 1: 0 marks "not split"
+                scratch_floats += need;
+            }
+        }
+        if (b->scratch_floats < scratch_floats) {
+            cudaFree(b->scratch);
+            b->scratch = nullptr;
+            b->scratch_floats = 0;
+            cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->scratch), scratch_floats * sizeof(float));
+            if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc view scratch");
+            b->scratch_floats = scratch_floats;
+        }
+    }
     for (uint32_t i = 0; i < n; ++i) {
         const SolGpuView& s = views[i];
         if (s.scene >= b->scenes.size()) return fail(SOL_GPU_ERR_INVALID_ARG, "view scene index out of range");
@@ -166,7 +204,11 @@ int upload_views(SolGpuBatch* b, const SolGpuView* views, uint32_t n, uint32_t* 
         w.film = s.film;
         w.tiles_x = (s.width + 7) / 8;
         w.item_begin = (uint32_t)items;
-        items += (uint64_t)w.tiles_x * ((s.height + 3) / 4) * 32;
+        w.split = scratch_at[i] != 0;
+        w.scratch = w.split ? b->scratch + (scratch_at[i] - 1) : nullptr;
+        w.sum_begin = sum_at;
+        if (w.split) sum_at += 3 * (uint64_t)s.width * s.height;
+        items += (uint64_t)w.tiles_x * ((s.height + 3) / 4) * 32 * (w.split ? s.sample_count : 1u);
         px += (uint64_t)s.width * s.height;
         if (items > 0xffffffffull) return fail(SOL_GPU_ERR_INVALID_ARG, "batch too large (more than 2^32 work items)");
     }
@@ -182,14 +224,39 @@ int upload_views(SolGpuBatch* b, const SolGpuView* views, uint32_t n, uint32_t* 
     if (e != cudaSuccess) return cuda_fail(e, "views upload");
     *total_items = (uint32_t)items;
     *pixels = px;
+    if (sum_floats) *sum_floats = sum_at;
     return SOL_GPU_OK;
 }
 
 int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* views, uint32_t n, cudaStream_t stream) {
     uint32_t total_items = 0;
-    uint64_t pixels = 0;
-    int rc = upload_views(b, views, n, &total_items, &pixels, stream);
+    uint64_t pixels = 0, sum_floats = 0;
+    const bool mk = b->opts.schedule == SOL_GPU_BATCH_MEGAKERNEL;
+    int rc = upload_views(b, views, n, &total_items, &pixels, stream, mk, &sum_floats);
     if (rc != SOL_GPU_OK) return rc;
+    if (mk) {
+        if (!b->d_dc) {
+            cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_dc), sizeof(DeviceCounters));
+            if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc counters");
+        }
+        uint32_t max_spp = 0;
+        for (uint32_t i = 0; i < n; ++i) max_spp = std::max(max_spp, views[i].sample_count);
+        const int per_sm = megakernel_views_blocks_per_sm();
+        if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
+        cudaError_t e = cudaMemsetAsync(b->d_dc, 0, sizeof(DeviceCounters), stream);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+        cudaEventRecord(b->ev_start, stream);
+        if (n > 0) {
+            e = launch_megakernel_views(b->d_views, n, total_items, max_spp, b->d_scenes, to_config(*config), b->d_dc,
+                                        b->scenes[0]->fault, per_sm * b->num_sms, stream);
+            if (e == cudaSuccess) e = launch_sum_samples_views(b->d_views, n, sum_floats, stream);
+            if (e != cudaSuccess) return cuda_fail(e, "megakernel launch");
+        }
+        cudaEventRecord(b->ev_stop, stream);
+        b->rendered = true;
+        b->last_dc = true;
+        return SOL_GPU_OK;
+    }
     uint32_t want = b->opts.capacity ? b->opts.capacity : kDefaultCapacity;
     want = std::min<uint32_t>(std::max<uint32_t>(want, 32), kMaxCapacity);
     rc = alloc_pool(b, want);
@@ -235,7 +302,7 @@ int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* v
     }
     cudaEventRecord(b->ev_stop, stream);
     b->rendered = true;
-    b->last_fused = false;
+    b->last_dc = false;
     return SOL_GPU_OK;
 }
 
@@ -264,6 +331,7 @@ bool read_cache(const char* path, const std::string& key, SolGpuBatchOptions* o)
         std::string k;
         SolGpuBatchOptions r{};
         if (std::getline(in, k, '\t') && (in >> r.capacity >> r.block_size >> r.sort_threshold) && k == key) {
+            if (!(in >> r.schedule)) r.schedule = SOL_GPU_BATCH_WAVEFRONT;
             *o = r;
             found = true;
         }
@@ -321,7 +389,8 @@ int sol_gpu_batch_destroy(SolGpuBatch* b) {
     cudaFree(b->d_scenes);
     cudaFree(b->d_views);
     cudaFree(b->d_adj_views);
-    cudaFree(b->d_fused_ctr);
+    cudaFree(b->d_dc);
+    cudaFree(b->scratch);
     if (b->h_ctr) cudaFreeHost(b->h_ctr);
     if (b->capture) cudaStreamDestroy(b->capture);
     if (b->ev_start) cudaEventDestroy(b->ev_start);
@@ -379,24 +448,24 @@ int sol_gpu_batch_forward_adjoint(SolGpuBatch* b, const SolGpuConfig* config, co
         if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc views");
         b->adj_views_cap = std::max<size_t>(n, 32);
     }
-    if (!b->d_fused_ctr) {
-        e = cudaMalloc(reinterpret_cast<void**>(&b->d_fused_ctr), sizeof(DeviceCounters));
+    if (!b->d_dc) {
+        e = cudaMalloc(reinterpret_cast<void**>(&b->d_dc), sizeof(DeviceCounters));
         if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc counters");
     }
     if (n > 0) e = cudaMemcpyAsync(b->d_adj_views, v.data(), sizeof(AdjView) * n, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_fused_ctr, 0, sizeof(DeviceCounters), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_dc, 0, sizeof(DeviceCounters), st);
     if (e != cudaSuccess) return cuda_fail(e, "fused batch upload");
     const int per_sm = fused_blocks_per_sm();
     if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "fused kernel occupancy query failed");
     cudaEventRecord(b->ev_start, st);
     if (n > 0) {
         e = launch_fused_forward_adjoint(b->d_adj_views, n, (uint32_t)items, b->d_scenes, to_config(*config),
-                                         b->d_fused_ctr, per_sm * b->num_sms, st);
+                                         b->d_dc, per_sm * b->num_sms, st);
         if (e != cudaSuccess) return cuda_fail(e, "fused forward/adjoint launch");
     }
     cudaEventRecord(b->ev_stop, st);
     b->rendered = true;
-    b->last_fused = true;
+    b->last_dc = true;
     return SOL_GPU_OK;
 }
 
@@ -407,12 +476,13 @@ int sol_gpu_batch_stats(SolGpuBatch* b, SolGpuRenderStats* out) {
     DeviceGuard guard(b->device);
     cudaError_t e = cudaEventSynchronize(b->ev_stop);
     if (e != cudaSuccess) return cuda_fail(e, "cudaEventSynchronize");
-    if (b->last_fused) {
+    if (b->last_dc) {
         DeviceCounters c;
-        e = cudaMemcpy(&c, b->d_fused_ctr, sizeof(c), cudaMemcpyDeviceToHost);
+        e = cudaMemcpy(&c, b->d_dc, sizeof(c), cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) return cuda_fail(e, "counters");
         out->paths = c.paths;
         out->rays = c.rays;
+        out->shadow_rays = c.shadow_rays;
     } else {
         WfCounters c;
         e = cudaMemcpy(&c, b->d_ctr, sizeof(c), cudaMemcpyDeviceToHost);
@@ -436,7 +506,12 @@ int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const Sol
     if (!b || !config || !views || num_views == 0) return fail(SOL_GPU_ERR_INVALID_ARG, "batch, config and views are required");
     DeviceGuard guard(b->device);
     if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
-    const std::string key = tune_key(b, views, num_views);
+    if (b->opts.schedule == SOL_GPU_BATCH_MEGAKERNEL) {   // nothing to choose
+        if (chosen) *chosen = b->opts;
+        return SOL_GPU_OK;
+    }
+    const bool both = b->opts.schedule == SOL_GPU_BATCH_AUTO;
+    const std::string key = tune_key(b, views, num_views) + (both ? "|auto" : "|wavefront");
     SolGpuBatchOptions best = b->opts;
     if (cache_path && read_cache(cache_path, key, &best)) {
         best.host_loop = b->opts.host_loop;
@@ -480,6 +555,24 @@ int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const Sol
             }
         }
     }
+    if (rc == SOL_GPU_OK) {
+        // Every candidate above ran as the wavefront; name it so.
+        best.schedule = SOL_GPU_BATCH_WAVEFRONT;
+    }
+    if (rc == SOL_GPU_OK && both) {
+        b->opts = saved;
+        b->opts.schedule = SOL_GPU_BATCH_MEGAKERNEL;
+        float ms = 0.0f;
+        for (int rep = 0; rep < 2 && rc == SOL_GPU_OK; ++rep) {
+            rc = render_batch(b, config, probe.data(), num_views, s);
+            if (rc == SOL_GPU_OK) {
+                e = cudaEventSynchronize(b->ev_stop);
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
+                if (e != cudaSuccess) rc = cuda_fail(e, "autotune timing");
+            }
+        }
+        if (rc == SOL_GPU_OK && ms < best_ms) { best_ms = ms; best = b->opts; }
+    }
     cudaFree(scratch);
     if (rc != SOL_GPU_OK) { b->opts = saved; return rc; }
     best.host_loop = saved.host_loop;
@@ -487,7 +580,8 @@ int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const Sol
     if (chosen) *chosen = best;
     if (cache_path) {
         std::ofstream f(cache_path, std::ios::app);
-        f << key << '\t' << best.capacity << ' ' << best.block_size << ' ' << best.sort_threshold << '\n';
+        f << key << '\t' << best.capacity << ' ' << best.block_size << ' ' << best.sort_threshold << ' '
+          << best.schedule << '\n';
     }
     return SOL_GPU_OK;
 }

@@ -28,6 +28,7 @@
 
 #include "kernels.h"
 #include "path.cuh"
+#include "wavefront.h"
 
 namespace sol_b200 {
 
@@ -168,6 +169,131 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
     }
 }
 
+/// K1b: the megakernel over many views (cameras, films of uneven size and spp)
+/// of one or more scenes in one persistent launch.  Work items are the views'
+/// 8x4 pixel tiles laid end to end (WfView::item_begin); a lane claims a pixel
+/// of any view, renders all its samples in order with path regeneration, adds
+/// the sum into that view's film and claims the next — the schedule of K1 with
+/// the view (scene, camera, film) looked up per pixel.  Split views (small
+/// images) have one item per (sample, pixel) as K1's split schedule does, and
+/// sum_samples_views adds their scratch planes afterwards, so every film has
+/// the bits a separate K1 launch gives it.
+template <bool kCount>
+__global__ void __launch_bounds__(kMegakernelBlock, kMegakernelMinBlocks)
+pt_megakernel_views(const WfView* __restrict__ views, uint32_t num_views, uint32_t total, uint32_t max_spp,
+                    const SceneView* __restrict__ scenes, DConfig cfg, DeviceCounters* __restrict__ ctr,
+                    unsigned int* __restrict__ fault) {
+    TraversalCounters tc{0u, 0u};
+    uint32_t n_paths = 0, n_rays = 0, n_shadow = 0;
+    LocalStack stack;
+    bool have_pixel = false;
+    uint32_t px = 0, py = 0, sample = 0, sample_end = 0, vi = 0;
+    Rgb pix_sum = rgb(0.0f);
+    PathState ps;
+    const SceneView* s = scenes;
+    float light_pick_prob = 1.0f;
+    bool done = false;
+    // Self-check bound: a lane claims at most every item, each with at most
+    // max_spp samples of at most max_path_len vertices.
+    const unsigned long long loop_bound = (unsigned long long)total * ((unsigned long long)max_spp + 1ull) *
+                                          ((unsigned long long)cfg.max_path_len + 1ull) + 64ull;
+    unsigned long long iterations = 0, claims = 0;
+    bool alive = false;
+
+    while (true) {
+        if (++iterations > loop_bound) { atomicOr(fault, kFaultPathLoop); break; }
+        while (!alive) {
+            if (++claims > loop_bound) { atomicOr(fault, kFaultClaimLoop); done = true; break; }
+            const WfView& V = views[vi];
+            if (have_pixel && sample < sample_end) {
+                DCamera cam;
+                for (int k = 0; k < 3; ++k) {
+                    cam.eye[k] = V.eye[k]; cam.dir[k] = V.dir[k]; cam.right[k] = V.right[k]; cam.up[k] = V.up[k];
+                }
+                start_path(ps, cam, V.sample_index + sample, px, py, V.width, V.height);
+                ++n_paths;
+                if (cfg.max_path_len == 0) { pix_sum = pix_sum + ps.color; ++sample; continue; }
+                alive = true;
+            } else {
+                if (have_pixel) {
+                    const size_t plane = (size_t)V.width * V.height;
+                    const size_t i = (size_t)py * V.width + px;
+                    if (V.split) {
+                        float* f = V.scratch + (size_t)(sample_end - 1u) * 3u * plane;
+                        f[i] = pix_sum.r;
+                        f[i + plane] = pix_sum.g;
+                        f[i + 2 * plane] = pix_sum.b;
+                    } else {
+                        // image.h:54-60 accumulate
+                        V.film[i] += pix_sum.r;
+                        V.film[i + plane] += pix_sum.g;
+                        V.film[i + 2 * plane] += pix_sum.b;
+                    }
+                    have_pixel = false;
+                }
+                const uint32_t item = claim_items(&ctr->next_item);
+                if (item >= total) { done = true; break; }
+                uint32_t lo = 0, hi = num_views;
+                while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (views[mid].item_begin <= item) lo = mid; else hi = mid; }
+                const WfView& W = views[lo];
+                uint32_t local = item - W.item_begin, k = 0;
+                if (W.split) {
+                    const uint32_t per_sample = W.tiles_x * ((W.height + 3u) / 4u) * 32u;
+                    k = local / per_sample;
+                    local -= k * per_sample;
+                }
+                const uint32_t tile = local >> 5, l = local & 31u;
+                px = (tile % W.tiles_x) * 8u + (l & 7u);
+                py = (tile / W.tiles_x) * 4u + (l >> 3);
+                if (px < W.width && py < W.height) {
+                    have_pixel = true;
+                    vi = lo;
+                    sample = k;
+                    sample_end = W.split ? k + 1u : W.sample_count;
+                    pix_sum = rgb(0.0f);
+                    s = scenes + W.scene;
+                    light_pick_prob = 1.0f / (float)s->num_lights;
+                }
+            }
+        }
+        if (done) break;
+
+        float t = kFloatMax;
+        const int slot = traverse<false, kCount>(*s, ps.org, ps.dir, ps.tmin, t, tc, stack);
+        ++n_rays;
+        VertexOut vo;
+        vo.has_shadow = false;
+        vo.end = slot < 0;
+        if (!vo.end) shade_vertex(*s, cfg, light_pick_prob, slot, t, ps, vo);
+        if (vo.has_shadow) {
+            float smax = 1.0f - cfg.ray_offset;
+            const int occ = traverse<true, kCount>(*s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc, stack);
+            ++n_rays;
+            ++n_shadow;
+            if (occ < 0) ps.color = ps.color + vo.pending;
+        }
+        bool end = vo.end;
+        if (!end) {
+            ++ps.path_len;
+            end = ps.path_len >= cfg.max_path_len;
+        }
+        if (end) {
+            pix_sum = pix_sum + ps.color;   // path_tracer.cpp:19
+            ++sample;
+            alive = false;
+        }
+    }
+    __syncwarp();
+    unsigned long long v0 = warp_sum_u64(n_paths), v1 = warp_sum_u64(n_rays), v2 = warp_sum_u64(n_shadow);
+    unsigned long long v3 = warp_sum_u64(tc.nodes), v4 = warp_sum_u64(tc.tris);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&ctr->paths, v0);
+        atomicAdd(&ctr->rays, v1);
+        atomicAdd(&ctr->shadow_rays, v2);
+        if (kCount) { atomicAdd(&ctr->nodes, v3); atomicAdd(&ctr->tris, v4); }
+    }
+}
+
 /// Adds each pixel's per-sample colours (scratch: sample_count x 3 planes) into
 /// the film in sample order, starting from 0 as the per-pixel loop does.
 __global__ void __launch_bounds__(256)
@@ -177,6 +303,26 @@ sum_samples(const float* __restrict__ scratch, uint32_t sample_count, size_t pla
         float sum = 0.0f;
         for (uint32_t k = 0; k < sample_count; ++k) sum += scratch[(size_t)k * n + i];
         film[i] += sum;
+    }
+}
+
+/// The sum pass of the split views of K1b: every float of those views' films
+/// (laid end to end from WfView::sum_begin) gets its pixel's per-sample colours
+/// added in sample order, starting from 0.
+__global__ void __launch_bounds__(256)
+sum_samples_views(const WfView* __restrict__ views, uint32_t num_views, uint64_t total) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total; g += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = num_views;
+        while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (views[mid].sum_begin <= g) lo = mid; else hi = mid; }
+        // Non-split views occupy no range: the last split view starting at or before g owns g.
+        while (lo > 0 && !views[lo].split) --lo;
+        if (!views[lo].split) continue;
+        const WfView& V = views[lo];
+        const size_t n = 3 * (size_t)V.width * V.height;
+        const size_t i = (size_t)(g - V.sum_begin);
+        float sum = 0.0f;
+        for (uint32_t k = 0; k < V.sample_count; ++k) sum += V.scratch[(size_t)k * n + i];
+        V.film[i] += sum;
     }
 }
 
@@ -198,6 +344,28 @@ cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DCon
         pt_megakernel<true, false><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, film, counters);
     else
         pt_megakernel<false, false><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, film, counters);
+    return cudaGetLastError();
+}
+
+int megakernel_views_blocks_per_sm() {
+    int n = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pt_megakernel_views<false>, kMegakernelBlock, 0) == cudaSuccess
+               ? n : -1;
+}
+
+cudaError_t launch_megakernel_views(const WfView* views, uint32_t num_views, uint32_t total_items, uint32_t max_spp,
+                                    const SceneView* scenes, const DConfig& cfg, DeviceCounters* counters,
+                                    unsigned int* fault, int grid, cudaStream_t stream) {
+    pt_megakernel_views<false><<<grid, kMegakernelBlock, 0, stream>>>(views, num_views, total_items, max_spp, scenes,
+                                                                       cfg, counters, fault);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, uint64_t total_floats,
+                                     cudaStream_t stream) {
+    if (total_floats == 0) return cudaSuccess;
+    const int blocks = (int)std::min<uint64_t>((total_floats + 255) / 256, 8192);
+    sum_samples_views<<<blocks, 256, 0, stream>>>(views, num_views, total_floats);
     return cudaGetLastError();
 }
 

@@ -9,6 +9,27 @@
 #include "../core/math.h"
 #include "../../../include/sol_gpu.h"
 
+// SOL_SHADE_OUTLINE = 1 keeps the texture lookup, the BSDF kinds and the light
+// sampling as single out-of-line copies (less code for the instruction cache,
+// at the price of calls); 0 lets the compiler inline them everywhere.
+#ifndef SOL_SHADE_OUTLINE
+#define SOL_SHADE_OUTLINE 0
+#endif
+#if SOL_SHADE_OUTLINE
+#define SOL_SHADE_FN __noinline__
+#else
+#define SOL_SHADE_FN inline
+#endif
+// SOL_TEX_OUTLINE = 1 keeps only the image-texture lookup out of line.
+#ifndef SOL_TEX_OUTLINE
+#define SOL_TEX_OUTLINE 0
+#endif
+#if SOL_TEX_OUTLINE || SOL_SHADE_OUTLINE
+#define SOL_TEX_FN __noinline__
+#else
+#define SOL_TEX_FN inline
+#endif
+
 namespace sol_b200 {
 
 // ---------------------------------------------------------------------------
@@ -27,7 +48,7 @@ __device__ __forceinline__ float fmod2_(float x) {
 }
 
 /// ImageTexture<Filter, Border>::sample_color (src/textures.cpp:47-52).
-__device__ inline Rgb image_color(const SceneView& s, const DTexture& t, Vec2 uv) {
+__device__ SOL_TEX_FN Rgb image_color(const SceneView& s, const DTexture& t, Vec2 uv) {
     // Border handling (textures.cpp:5-21); Mirror uses uv[0] for both axes as SoL does.
     if (t.border == SOL_GPU_BORDER_CLAMP) {
         uv = vec2(clampf(uv.x, 0.0f, 1.0f), clampf(uv.y, 0.0f, 1.0f));
@@ -113,7 +134,7 @@ __device__ __forceinline__ Rgb phong_eval(Vec3 in_dir, const Surface& sf, Vec3 o
 }
 
 /// Bsdf::eval for the non-interpolating kinds (Mirror and Glass return black).
-__device__ inline Rgb bsdf_eval_basic(const SceneView& s, const DBsdf& b, Vec3 in_dir, const Surface& sf, Vec3 out_dir) {
+__device__ SOL_SHADE_FN Rgb bsdf_eval_basic(const SceneView& s, const DBsdf& b, Vec3 in_dir, const Surface& sf, Vec3 out_dir) {
     if (b.kind == SOL_GPU_BSDF_DIFFUSE)                       // bsdfs.cpp:35-37
         return tex_color(s, b.tex[0], sf.uv) * kInvPi;
     if (b.kind == SOL_GPU_BSDF_PHONG)                         // bsdfs.cpp:68-70
@@ -122,7 +143,7 @@ __device__ inline Rgb bsdf_eval_basic(const SceneView& s, const DBsdf& b, Vec3 i
 }
 
 /// Bsdf::pdf for the non-interpolating kinds (Mirror and Glass return 0).
-__device__ inline float bsdf_pdf_basic(const SceneView& s, const DBsdf& b, Vec3 in_dir, const Surface& sf, Vec3 out_dir) {
+__device__ SOL_SHADE_FN float bsdf_pdf_basic(const SceneView& s, const DBsdf& b, Vec3 in_dir, const Surface& sf, Vec3 out_dir) {
     if (b.kind == SOL_GPU_BSDF_DIFFUSE)                       // bsdfs.cpp:50-52
         return cosine_hemisphere_pdf(positive_dot(in_dir, sf.normal()));
     if (b.kind == SOL_GPU_BSDF_PHONG)                         // bsdfs.cpp:87-89
@@ -162,7 +183,7 @@ __device__ __forceinline__ bool validate(const Surface& sf, const BsdfSample& bs
 }
 
 /// Bsdf::sample for the non-interpolating kinds.
-__device__ inline bool bsdf_sample_basic(const SceneView& s, const DBsdf& b, Pcg& rng, const Surface& sf,
+__device__ SOL_SHADE_FN bool bsdf_sample_basic(const SceneView& s, const DBsdf& b, Pcg& rng, const Surface& sf,
                                   Vec3 out_dir, BsdfSample* out) {
     if (b.kind == SOL_GPU_BSDF_DIFFUSE) {
         // bsdfs.cpp:39-48; sample_cosine_hemisphere(sampler(), sampler()): v drawn first
@@ -256,7 +277,7 @@ __device__ __forceinline__ Vec3 ld3(const float* p) { return vec3(p[0], p[1], p[
 
 /// Light::sample_area for the three light kinds (lights.cpp:15-24, 64-77;
 /// shapes.cpp:13-16, 20-25, 33-37).
-__device__ inline bool light_sample_area(const SceneView& s, const DLight& l, Pcg& rng, Vec3 from, LightSample* out) {
+__device__ SOL_SHADE_FN bool light_sample_area(const SceneView& s, const DLight& l, Pcg& rng, Vec3 from, LightSample* out) {
     if (l.kind == SOL_GPU_LIGHT_POINT) {
         out->pos = ld3(l.v0);
         out->intensity = rgb(l.intensity[0], l.intensity[1], l.intensity[2]);
@@ -290,7 +311,7 @@ __device__ inline bool light_sample_area(const SceneView& s, const DLight& l, Pc
 
 /// Light::emission at a hit point seen along `dir` (pointing away from the
 /// light), lights.cpp:38-40, 94-106.  Returns the intensity and pdf_from.
-__device__ inline void light_emission(const SceneView& s, const DLight& l, Vec3 dir, Vec2 uv, Rgb* intensity, float* pdf_from) {
+__device__ SOL_SHADE_FN void light_emission(const SceneView& s, const DLight& l, Vec3 dir, Vec2 uv, Rgb* intensity, float* pdf_from) {
     if (l.kind == SOL_GPU_LIGHT_POINT) { *intensity = rgb(0.0f); *pdf_from = 1.0f; return; }
     Vec3 n;
     if (l.kind == SOL_GPU_LIGHT_TRIANGLE) {

@@ -21,7 +21,7 @@ constexpr int kWfBins = 6;
 constexpr int kWfRefillBelow = SOL_WF_REFILL_BELOW;
 
 #ifndef SOL_WF_TRACE_MIN_BLOCKS
-#define SOL_WF_TRACE_MIN_BLOCKS 1
+#define SOL_WF_TRACE_MIN_BLOCKS 5
 #endif
 /// Resident 256-thread blocks per SM the traversal stages' registers must allow.
 constexpr int kWfTraceMinBlocks = SOL_WF_TRACE_MIN_BLOCKS;
@@ -36,6 +36,12 @@ struct WfView {
     float* film;             // device film, 3 planes of width*height, +=
     uint32_t item_begin;     // first work item of this view (8x4 pixel tiles, 32 items each)
     uint32_t tiles_x;
+    // Multi-view megakernel only: split views have one work item per (sample,
+    // pixel) and write each sample's colour to `scratch` (sample_count x 3
+    // planes); `sum_begin` is the view's first float in the sum pass.
+    uint32_t split;
+    float* scratch;
+    uint64_t sum_begin;
 };
 
 struct WfCounters {

@@ -1,6 +1,7 @@
-"""Batched wavefront renderer (generate / extend / shade / shadow stages, CUDA-graph
-bounce loop): every view's film must equal what the per-view megakernel adds for
-the same camera and sample range, bit for bit, and match the CPU checker."""
+"""Batched renderer, both schedules: the wavefront (generate / extend / shade /
+shadow stages, CUDA-graph bounce loop) and the persistent multi-view megakernel.
+Every view's film must equal what the per-view megakernel adds for the same
+camera and sample range, bit for bit, and match the CPU checker."""
 import numpy as np
 import pytest
 
@@ -46,7 +47,7 @@ def _render_both(scenes, specs, cfg, **opts):
 
 
 @pytest.mark.parametrize("opts", [dict(), dict(capacity=4096, block_size=64), dict(sort_threshold=0xFFFFFFFF),
-                                  dict(host_loop=True, block_size=256)])
+                                  dict(host_loop=True, block_size=256), dict(schedule=1)])
 def test_batch_equals_megakernel_cornell(built, opts):
     from sol_b200 import scenes
     scene = scenes.cornell_box(0)
@@ -57,14 +58,15 @@ def test_batch_equals_megakernel_cornell(built, opts):
     assert st.paths == sum(w * h * spp for (_, _, w, h, _, spp) in specs)
 
 
-def test_batch_multi_scene_matches_oracle(built):
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_batch_multi_scene_matches_oracle(built, schedule):
     from sol_b200 import scenes
     sc = [scenes.cornell_box(0), scenes.sphere_field(5, seed=7, bands=17, segments=32),
           scenes.cornell_box(1, textured=True, tex_size=32)]
     specs = []
     for si, s in enumerate(sc):
         specs += [(si,) + v for v in _views(s, 3, seed=10 + si, max_side=40, max_spp=3)]
-    b, m, _ = _render_both(sc, specs, scenes.CORNELL_CONFIG)
+    b, m, _ = _render_both(sc, specs, scenes.CORNELL_CONFIG, schedule=schedule)
     for (si, cam, w, h, idx, spp), fb, fm in zip(specs, b, m):
         assert np.array_equal(fb, fm)
         o = oracle.render(sc[si], scenes.CORNELL_CONFIG, w, h, spp, sample_index=idx, camera=cam,
@@ -90,3 +92,27 @@ def test_autotune_picks_and_caches(built, tmp_path):
     assert (again.capacity, again.block_size, again.sort_threshold) == (chosen.capacity, chosen.block_size,
                                                                          chosen.sort_threshold)
     assert all(float(f.abs().sum()) == 0.0 for f in films)   # tuning renders into scratch films
+
+
+def test_autotune_auto_chooses_a_schedule(built, tmp_path):
+    """With schedule AUTO the tuner also times the megakernel schedule and
+    reports the winner explicitly; rendering with it keeps the films' bits."""
+    import torch
+    from sol_b200 import capi, scenes
+    from sol_b200.renderer import BatchRenderer, GpuPathTracer, GpuScene
+    scene = scenes.cornell_box(0)
+    gs = GpuScene(scene)
+    specs = [(scene.camera, 48, 40, 3, 5), (scene.camera, 20, 64, 100, 2)]
+    films = [torch.zeros((3, h, w), device="cuda") for (_, w, h, _, _) in specs]
+    br = BatchRenderer([gs], schedule=capi.BATCH_AUTO)
+    views = br.views([(0, cam, w, h, idx, spp, f.data_ptr()) for (cam, w, h, idx, spp), f in zip(specs, films)])
+    chosen = br.autotune(scenes.CORNELL_CONFIG, views, str(tmp_path / "tune.txt"))
+    assert chosen.schedule in (capi.BATCH_WAVEFRONT, capi.BATCH_MEGAKERNEL)
+    br.render(scenes.CORNELL_CONFIG, views, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    for (cam, w, h, idx, spp), f in zip(specs, films):
+        ref = torch.zeros_like(f)
+        GpuPathTracer(gs, scenes.CORNELL_CONFIG, camera=cam).render_device(ref.data_ptr(), w, h, idx, spp,
+                                                                          torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert torch.equal(f, ref)
