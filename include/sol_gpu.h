@@ -328,6 +328,43 @@ int sol_gpu_batch_stats(SolGpuBatch* batch, SolGpuRenderStats* out);
 int sol_gpu_batch_autotune(SolGpuBatch* batch, const SolGpuConfig* config, const SolGpuView* views,
                            uint32_t num_views, const char* cache_path, SolGpuBatchOptions* chosen);
 
+/* ---- Progressive rendering job ---------------------------------------------
+ *
+ * The GPU counterpart of sol::RenderJob (include/sol/render_job.h,
+ * src/render_job.cpp:23-59): frames of samples rendered on a host thread into
+ * a device copy of the caller's film, which is copied back into the caller's
+ * planes after every frame.  Frames cover the sample ranges SoL's RenderJob
+ * gives them (render_job.cpp:27-31), so with the same renderer the film
+ * matches sol::RenderJob's bit for bit. */
+
+typedef struct SolGpuJob SolGpuJob;
+
+/* Called on the job's thread after each frame, once the host film holds the
+ * image so far; `frames` counts the frames done.  Return 0 to stop the job. */
+typedef int (*SolGpuFrameEnd)(void* user, uint64_t frames);
+
+/* Starts rendering samples into film_r/g/b (host planes of width*height,
+ * added into like sol_gpu_render); sample_count 0 renders until cancelled.
+ * The film must stay valid and untouched by the caller until the job has
+ * finished (sol_gpu_job_wait), except inside frame_end. */
+int sol_gpu_job_start(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config, uint32_t width,
+                      uint32_t height, float* film_r, float* film_g, float* film_b, uint64_t sample_count,
+                      uint32_t samples_per_frame, SolGpuFrameEnd frame_end, void* user, SolGpuJob** out);
+
+/* RenderJob::wait: waits for the job to end, at most timeout_ms milliseconds
+ * (0 = no limit); *finished = 1 when it has ended.  Returns the status of the
+ * job's renders once it has ended. */
+int sol_gpu_job_wait(SolGpuJob* job, uint32_t timeout_ms, int* finished);
+
+/* RenderJob::cancel: the job stops after the frame in flight. */
+int sol_gpu_job_cancel(SolGpuJob* job);
+
+/* Frames finished so far. */
+int sol_gpu_job_frames(const SolGpuJob* job, uint64_t* frames);
+
+/* Cancels, waits for the job and frees it. */
+int sol_gpu_job_destroy(SolGpuJob* job);
+
 /* ---- Differentiation --------------------------------------------------------
  *
  * Parameters are the scene's texture values: for each texture in order, a

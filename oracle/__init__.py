@@ -11,6 +11,7 @@ Only tests, the smoke check and bench.py's CPU-baseline leg use this package.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -19,7 +20,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "_build" / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libsol_ref.so"
-REF_SOURCES = Path("/root/reference")
+# SoL's source tree (read only); SOL_REFERENCE_DIR points elsewhere (e.g. a copy of its test scenes).
+REF_SOURCES = Path(os.environ.get("SOL_REFERENCE_DIR", "/root/reference"))
 
 _oracle = None
 _ref = None
@@ -85,6 +87,16 @@ def ref_available() -> bool:
     return REF_LIB.exists()
 
 
+REFERENCE_SCENES = ("cornell_box", "cornell_box_glossy", "cornell_box_specular", "cornell_box_water")
+
+
+def reference_scene(name: str):
+    """Path of one of SoL's own test scene files (test/data/<name>.toml), or None
+    where SoL's sources are not present."""
+    p = REF_SOURCES / "test" / "data" / f"{name}.toml"
+    return p if p.exists() else None
+
+
 def ref_lib() -> C.CDLL:
     global _ref
     if _ref is None:
@@ -110,6 +122,10 @@ def ref_lib() -> C.CDLL:
         lib.ref_renderjob_render.restype = C.c_int
         lib.ref_last_error.argtypes = []
         lib.ref_last_error.restype = C.c_char_p
+        lib.ref_scene_load.argtypes = [C.c_char_p, C.c_float]
+        lib.ref_scene_load.restype = C.c_void_p
+        lib.ref_scene_counts.argtypes = [C.c_void_p] + [C.POINTER(C.c_uint32)] * 4
+        lib.ref_scene_counts.restype = None
         _ref = lib
     return _ref
 
@@ -176,12 +192,30 @@ class RefScene:
     """A sol::Scene built by SoL's own constructors, rendered by sol::PathTracer."""
 
     def __init__(self, scene, camera=None):
+        self.lib = ref_lib()
+        if scene is None:   # filled in by load()
+            self.h = None
+            return
         self._desc = scene.desc()
         cam = camera_args(camera or scene.camera)
-        self.lib = ref_lib()
         self.h = self.lib.ref_scene_create(self._desc.ptr, C.byref(cam))
         if not self.h:
             raise RuntimeError("ref_scene_create failed: " + self.lib.ref_last_error().decode())
+
+    @classmethod
+    def load(cls, path: str, aspect_ratio: float = 1.0) -> "RefScene":
+        """A scene file loaded by SoL's own loader (sol::Scene::load)."""
+        rs = cls(None)
+        rs.h = rs.lib.ref_scene_load(str(path).encode(), aspect_ratio)
+        if not rs.h:
+            raise RuntimeError("sol::Scene::load failed: " + rs.lib.ref_last_error().decode())
+        return rs
+
+    def counts(self) -> dict:
+        """Sizes of the scene's light, BSDF, texture and image tables."""
+        v = [C.c_uint32() for _ in range(4)]
+        self.lib.ref_scene_counts(self.h, *[C.byref(x) for x in v])
+        return dict(zip(("lights", "bsdfs", "textures", "images"), (x.value for x in v)))
 
     def render(self, config, width, height, spp, sample_index=0, threads=0, film=None):
         """Returns (film, render_ms)."""

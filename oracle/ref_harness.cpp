@@ -9,6 +9,7 @@
 #include <cstring>
 #include <memory>
 #include <optional>
+#include <sstream>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -141,6 +142,32 @@ RefScene* ref_scene_create(const SolGpuSceneDesc* d, const OracleCamera* cam) {
 }
 
 void ref_scene_destroy(RefScene* s) { delete s; }
+
+/// A scene file loaded by SoL's own loader (sol::Scene::load, src/scene_loader.cpp:
+/// TOML scene description + OBJ/MTL import, src/formats/obj.cpp), with the
+/// camera's aspect ratio defaulting to `aspect_ratio` as test/driver.cpp:197-199
+/// sets it.  Returns nullptr with the loader's message in ref_last_error().
+RefScene* ref_scene_load(const char* path, float aspect_ratio) {
+    try {
+        sol::Scene::Defaults defaults;
+        defaults.aspect_ratio = aspect_ratio;
+        std::ostringstream err;
+        auto scene = sol::Scene::load(path, defaults, &err);
+        if (!scene) { g_err = err.str(); return nullptr; }
+        return new RefScene{std::move(*scene)};
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+
+/// Sizes of a loaded scene's tables: lights, BSDFs, textures, images.
+void ref_scene_counts(const RefScene* rs, uint32_t* lights, uint32_t* bsdfs, uint32_t* textures, uint32_t* images) {
+    *lights = (uint32_t)rs->scene.lights.size();
+    *bsdfs = (uint32_t)rs->scene.bsdfs.size();
+    *textures = (uint32_t)rs->scene.textures.size();
+    *images = (uint32_t)rs->scene.images.size();
+}
 
 /// sol::PathTracer::render on a film that starts as the caller's channels and
 /// is copied back afterwards (so the caller sees SoL's `+=`).  Returns the time

@@ -24,7 +24,7 @@ LIB = LIB_DIR / "libsol_gpu.so"
 
 CUDA_SOURCES = ["kernels/megakernel.cu", "kernels/trace.cu", "kernels/wavefront.cu", "kernels/adjoint.cu",
                 "noalloc.cu"]
-HOST_SOURCES = ["capi.cpp", "batch.cpp", "host/flatten.cpp"]
+HOST_SOURCES = ["capi.cpp", "batch.cpp", "job.cpp", "host/flatten.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_DEVICE = ARCH + ["-O3", "-lineinfo", "-std=c++20", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",

@@ -114,6 +114,8 @@ class SolGpuBatchOptions(C.Structure):
 
 ScenePtr = C.c_void_p
 BatchPtr = C.c_void_p
+JobPtr = C.c_void_p
+FrameEnd = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_uint64)
 
 # (name, restype, argtypes) of every entry point declared in include/sol_gpu.h
 SIGNATURES = [
@@ -151,6 +153,13 @@ SIGNATURES = [
     ("sol_gpu_adjoint", C.c_int, [ScenePtr, C.POINTER(SolGpuCamera), C.POINTER(SolGpuConfig), C.c_uint64, C.c_uint32,
                                   C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("sol_gpu_image_l2", C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("sol_gpu_job_start", C.c_int, [ScenePtr, C.POINTER(SolGpuCamera), C.POINTER(SolGpuConfig), C.c_uint32, C.c_uint32,
+                                     f32p, f32p, f32p, C.c_uint64, C.c_uint32, FrameEnd, C.c_void_p,
+                                     C.POINTER(JobPtr)]),
+    ("sol_gpu_job_wait", C.c_int, [JobPtr, C.c_uint32, C.POINTER(C.c_int)]),
+    ("sol_gpu_job_cancel", C.c_int, [JobPtr]),
+    ("sol_gpu_job_frames", C.c_int, [JobPtr, C.POINTER(C.c_uint64)]),
+    ("sol_gpu_job_destroy", C.c_int, [JobPtr]),
     ("sol_gpu_build_bvh", C.c_int, [f32p, C.c_uint32, u32p, C.c_uint32, C.POINTER(SolGpuBvhNode), u32p, u32p]),
 ]
 

@@ -16,7 +16,7 @@
 #define SOL_SHADE_OUTLINE 0
 #endif
 #if SOL_SHADE_OUTLINE
-#define SOL_SHADE_FN __noinline__
+#define SOL_SHADE_FN inline __noinline__
 #else
 #define SOL_SHADE_FN inline
 #endif
@@ -25,7 +25,7 @@
 #define SOL_TEX_OUTLINE 0
 #endif
 #if SOL_TEX_OUTLINE || SOL_SHADE_OUTLINE
-#define SOL_TEX_FN __noinline__
+#define SOL_TEX_FN inline __noinline__
 #else
 #define SOL_TEX_FN inline
 #endif

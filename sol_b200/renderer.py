@@ -41,6 +41,24 @@ class Image:
     def rgb_at(self, x: int, y: int):
         return tuple(float(self.channels[c, y, x]) for c in range(3))
 
+    def save(self, path: str) -> None:
+        """Image::save for OpenEXR (src/image.cpp:25-36, src/formats/exr.cpp:47-100):
+        float channels named B, G, R.  Other formats are not written here."""
+        if not str(path).lower().endswith(".exr"):
+            raise ValueError("only .exr output is supported")
+        from .film import save_exr
+        save_exr(str(path), self.channels)
+
+    @classmethod
+    def load(cls, path: str) -> "Image":
+        """Reads an EXR written by save() (R, G, B planes back in SoL's order)."""
+        from .film import load_exr
+        planes, names = load_exr(str(path))
+        img = cls(planes.shape[2], planes.shape[1])
+        for c, name in enumerate("RGB"):
+            img.channels[c] = planes[names.index(name)]
+        return img
+
 
 class GpuScene:
     """A scene uploaded to one GPU. `bvh` optionally passes a prebuilt BVH (see scene.build_bvh)."""
@@ -147,6 +165,76 @@ class GpuPathTracer:
         out = capi.SolGpuRenderStats()
         capi.check(capi.lib.sol_gpu_render_stats(self.scene.handle, C.byref(out)), "sol_gpu_render_stats")
         return out
+
+
+class GpuRenderJob:
+    """sol::RenderJob on the GPU (include/sol/render_job.h): frames of
+    `samples_per_frame` samples added into `output` on a background thread.
+    start(frame_end) takes an optional callable(job) -> bool called after each
+    frame with `output` up to date; False stops the job."""
+
+    def __init__(self, renderer: "GpuPathTracer", output: Image):
+        self.renderer = renderer
+        self.output = output
+        self.sample_count = 0
+        self.samples_per_frame = 1
+        self.handle = None
+        self._cb = None
+        self._frames = 0
+
+    def start(self, frame_end=None) -> None:
+        if self.handle:
+            raise RuntimeError("job already started")
+        ch = self.output.channels
+        if not ch.flags.c_contiguous or ch.dtype != np.float32:
+            raise ValueError("image channels must be C-contiguous float32")
+
+        def trampoline(_user, frames):
+            self._frames = int(frames)
+            try:
+                return 1 if frame_end is None or frame_end(self) else 0
+            except Exception:
+                return 0
+        self._cb = capi.FrameEnd(trampoline)
+        f32p = C.POINTER(C.c_float)
+        h = capi.JobPtr()
+        r = self.renderer
+        capi.check(capi.lib.sol_gpu_job_start(r.scene.handle, C.byref(r._cam), C.byref(r._cfg), self.output.width,
+                                              self.output.height, *[ch[c].ctypes.data_as(f32p) for c in range(3)],
+                                              int(self.sample_count), int(self.samples_per_frame), self._cb, None,
+                                              C.byref(h)), "sol_gpu_job_start")
+        self.handle = h
+
+    def wait(self, timeout_ms: int = 0) -> bool:
+        if not self.handle:
+            return True
+        done = C.c_int(0)
+        capi.check(capi.lib.sol_gpu_job_wait(self.handle, int(timeout_ms), C.byref(done)), "sol_gpu_job_wait")
+        return bool(done.value)
+
+    def cancel(self) -> None:
+        if self.handle:
+            capi.check(capi.lib.sol_gpu_job_cancel(self.handle), "sol_gpu_job_cancel")
+
+    @property
+    def frames(self) -> int:
+        """Frames finished so far (inside frame_end: including the one just finished)."""
+        if not self.handle:
+            return self._frames
+        n = C.c_uint64(0)
+        capi.check(capi.lib.sol_gpu_job_frames(self.handle, C.byref(n)), "sol_gpu_job_frames")
+        return max(n.value, self._frames)
+
+    def close(self) -> None:
+        if self.handle:
+            capi.lib.sol_gpu_job_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def image_l2(film_ptr: int, target_ptr: int, count: int, film_scale: float, dl_dfilm_ptr: int, loss_ptr: int,
