@@ -84,7 +84,7 @@ void release(SolGpuScene* s) {
     DeviceGuard g(s->device);
     cudaFree(s->nodes); cudaFree(s->tris); cudaFree(s->shade); cudaFree(s->bsdfs);
     cudaFree(s->textures); cudaFree(s->images); cudaFree(s->texels); cudaFree(s->lights);
-    cudaFree(s->counters); cudaFree(s->film_tmp); cudaFree(s->split_scratch); cudaFree(s->param_offsets); cudaFree(s->fault);
+    cudaFree(s->counters); cudaFree(s->film_tmp); cudaFree(s->split_scratch); cudaFree(s->adj_texels4); cudaFree(s->param_offsets); cudaFree(s->fault);
     if (s->film_host) cudaFreeHost(s->film_host);
     if (s->ev_start) cudaEventDestroy(s->ev_start);
     if (s->ev_stop) cudaEventDestroy(s->ev_stop);
@@ -435,8 +435,19 @@ int sol_gpu_adjoint(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpu
     chunks = std::max<uint64_t>(1, std::min<uint64_t>(chunks, 0x7fffffffull / total));
     const uint32_t chunk = (uint32_t)((sample_count + chunks - 1) / chunks);
     cudaEventRecord(scene->ev_start, st);
+    const uint64_t num_texels = scene->texel_count / 3;
+    if (num_texels > scene->adj_texels4_count) {
+        cudaFree(scene->adj_texels4);
+        scene->adj_texels4 = nullptr;
+        scene->adj_texels4_count = 0;
+        e = cudaMalloc(reinterpret_cast<void**>(&scene->adj_texels4), sizeof(float4) * num_texels);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc texel gradient scratch");
+        scene->adj_texels4_count = num_texels;
+    }
     e = launch_adjoint(scene->view, to_camera(*camera), to_config(*config), sample_index, sample_count, chunk, width,
-                       height, dl_dfilm, grad, n_shared, scene->counters, per_sm * scene->num_sms, st);
+                       height, dl_dfilm, grad, n_shared, scene->adj_texels4, num_texels,
+                       (uint32_t)scene->host_images.size(), scene->constants_count, scene->counters,
+                       per_sm * scene->num_sms, st);
     if (e != cudaSuccess) return cuda_fail(e, "adjoint launch");
     cudaEventRecord(scene->ev_stop, st);
     scene->rendered = true;

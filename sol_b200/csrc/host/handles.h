@@ -25,6 +25,8 @@ struct SolGpuScene {
     sol_b200::DeviceCounters* counters = nullptr;
     unsigned int* fault = nullptr;   // kFault* bits set by the kernels' self-checks
     float* split_scratch = nullptr;  // per-sample colours of split-schedule renders
+    float4* adj_texels4 = nullptr;   // interleaved texel gradients of sol_gpu_adjoint
+    uint64_t adj_texels4_count = 0;
     size_t split_floats = 0;
     float* film_tmp = nullptr;       // device film for host-film renders
     size_t film_tmp_floats = 0;

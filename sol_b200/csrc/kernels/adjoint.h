@@ -61,9 +61,13 @@ cudaError_t launch_fused_forward_adjoint(const AdjView* views, uint32_t num_view
 /// work item replays `chunk` consecutive samples of one pixel; the first
 /// `n_shared` parameters (at most kAdjointMaxSharedParams, all of them constant
 /// textures) are gathered per block in shared memory.
+/// With `texels4` (num_texels float4, one per image texel in arena order) the
+/// image-texel gradients are gathered there with vector reductions and added
+/// into `grad` afterwards (parameter first_texel_param + image offset + ...).
 cudaError_t launch_adjoint(const SceneView& s, const DCamera& cam, const DConfig& cfg, uint64_t sample_index,
                            uint32_t sample_count, uint32_t chunk, uint32_t width, uint32_t height,
-                           const float* dl_dfilm, float* grad, uint32_t n_shared, DeviceCounters* counters, int grid,
+                           const float* dl_dfilm, float* grad, uint32_t n_shared, float4* texels4, uint64_t num_texels,
+                           uint32_t num_images, uint64_t first_texel_param, DeviceCounters* counters, int grid,
                            cudaStream_t stream);
 
 /// Adds sum (scale * film - target)^2 into *loss and writes dL/dfilm (optional).
