@@ -9,7 +9,7 @@
 namespace sol_b200 {
 
 #ifndef SOL_ADJOINT_MIN_BLOCKS
-#define SOL_ADJOINT_MIN_BLOCKS 6   // resident blocks per SM the register allocation must allow (80 registers; measured fastest)
+#define SOL_ADJOINT_MIN_BLOCKS 16  // resident blocks per SM the register allocation must allow (32 registers; measured fastest)
 #endif
 constexpr int kAdjointBlock = 128;
 constexpr int kAdjointMinBlocks = SOL_ADJOINT_MIN_BLOCKS;
@@ -46,7 +46,7 @@ inline uint64_t fused_items(uint32_t width, uint32_t height, uint32_t spp) {
 }
 
 /// Most constant-texture values whose gradients a block gathers in shared memory.
-constexpr uint32_t kAdjointMaxSharedParams = 8192;
+constexpr uint32_t kAdjointMaxSharedParams = 2048;   // 8 KB per block, so 16 blocks fit an SM
 
 int adjoint_blocks_per_sm(uint32_t n_shared);
 int fused_blocks_per_sm();
