@@ -248,7 +248,8 @@ int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* v
         cudaEventRecord(b->ev_start, stream);
         if (n > 0) {
             e = launch_megakernel_views(b->d_views, n, total_items, max_spp, b->d_scenes, to_config(*config), b->d_dc,
-                                        b->scenes[0]->fault, per_sm * b->num_sms, stream);
+                                        b->scenes[0]->fault, per_sm * b->num_sms, stream,
+                                        b->scenes.size() == 1 ? b->scenes[0]->l2 : L2Window{});
             if (e == cudaSuccess) e = launch_sum_samples_views(b->d_views, n, sum_floats, stream);
             if (e != cudaSuccess) return cuda_fail(e, "megakernel launch");
         }

@@ -133,10 +133,11 @@ int render_into(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConf
     cudaEventRecord(scene->ev_start, stream);
     if (split)
         e = launch_megakernel_split(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
-                                    scene->split_scratch, scene->counters, scene->instrumented, grid, stream);
+                                    scene->split_scratch, scene->counters, scene->instrumented, grid, stream,
+                                    scene->l2);
     else
         e = launch_megakernel(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
-                              scene->counters, scene->instrumented, grid, stream);
+                              scene->counters, scene->instrumented, grid, stream, scene->l2);
     if (e != cudaSuccess) return cuda_fail(e, "megakernel launch");
     cudaEventRecord(scene->ev_stop, stream);
     scene->rendered = true;
@@ -229,6 +230,29 @@ int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** 
     s->info.device_bytes = flat.nodes.size() * sizeof(DNode) + flat.tris.size() * sizeof(DTri) +
                            flat.shade.size() * sizeof(DTriShade);
     s->info.build_ms = (float)flat.build_ms;
+#if SOL_L2_PERSIST
+    // Keep the upper BVH levels (stored first) in L2: raise this process's
+    // persisting-L2 carve-out up to the device maximum if the range needs it,
+    // and let the render launches mark that range as persisting.
+    {
+        int max_persist = 0;
+        if (cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, s->device) == cudaSuccess &&
+            max_persist > 0) {
+            const size_t want = std::min<size_t>((size_t)flat.top_nodes * sizeof(DNode), (size_t)max_persist);
+            size_t have = 0;
+            cudaDeviceGetLimit(&have, cudaLimitPersistingL2CacheSize);
+            if (want > have) cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want);
+            cudaDeviceGetLimit(&have, cudaLimitPersistingL2CacheSize);
+            const size_t bytes = (size_t)flat.top_nodes * sizeof(DNode);
+            if (have > 0 && bytes > 0) {
+                s->l2.base = s->nodes;
+                s->l2.bytes = bytes;
+                s->l2.hit_ratio = (float)std::min(1.0, (double)have / (double)bytes);
+            }
+        }
+        cudaGetLastError();   // a device without persisting L2 simply runs without the window
+    }
+#endif
     *out = s;
     return SOL_GPU_OK;
 }

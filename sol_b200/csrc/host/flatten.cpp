@@ -241,16 +241,36 @@ bool flatten_scene(const SolGpuSceneDesc& d, FlatScene& out, std::string& err) {
             put_box(g, 0, tree.nodes[0].box); put_box(g, 1, tree.nodes[0].box);
             g.ref[0] = g.ref[1] = ref_of(0);
             out.nodes.push_back(g);
+            out.top_nodes = 1;
         } else {
+            // Upper levels breadth first (whole levels while they fit in
+            // kTopNodesMax), then every remaining subtree depth first (left
+            // first).  Only the storage order changes: node 0 is the root and
+            // each node keeps its children in the same order.
             std::vector<uint32_t> order;
-            std::vector<uint32_t> stack{0};
-            while (!stack.empty()) {
-                uint32_t i = stack.back(); stack.pop_back();
-                gpu_index[i] = (int32_t)order.size();
-                order.push_back(i);
-                const bvh::Node& n = tree.nodes[i];
-                if (!tree.nodes[n.first + 1].is_leaf()) stack.push_back(n.first + 1);
-                if (!tree.nodes[n.first].is_leaf()) stack.push_back(n.first);
+            std::vector<uint32_t> level{0};
+            while (!level.empty() && order.size() + level.size() <= kTopNodesMax) {
+                std::vector<uint32_t> next;
+                for (uint32_t i : level) {
+                    gpu_index[i] = (int32_t)order.size();
+                    order.push_back(i);
+                    const bvh::Node& n = tree.nodes[i];
+                    if (!tree.nodes[n.first].is_leaf()) next.push_back(n.first);
+                    if (!tree.nodes[n.first + 1].is_leaf()) next.push_back(n.first + 1);
+                }
+                level.swap(next);
+            }
+            out.top_nodes = (uint32_t)order.size();
+            for (uint32_t root : level) {
+                std::vector<uint32_t> stack{root};
+                while (!stack.empty()) {
+                    uint32_t i = stack.back(); stack.pop_back();
+                    gpu_index[i] = (int32_t)order.size();
+                    order.push_back(i);
+                    const bvh::Node& n = tree.nodes[i];
+                    if (!tree.nodes[n.first + 1].is_leaf()) stack.push_back(n.first + 1);
+                    if (!tree.nodes[n.first].is_leaf()) stack.push_back(n.first);
+                }
             }
             out.nodes.resize(order.size());
             for (size_t k = 0; k < order.size(); ++k) {

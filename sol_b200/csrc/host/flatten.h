@@ -10,6 +10,11 @@
 
 namespace sol_b200 {
 
+/// Inner nodes of the upper BVH levels stored first, level by level, so that
+/// one contiguous range of the node array can be kept resident in L2: whole
+/// levels are taken while they fit in this many nodes (64 B each, 16 MiB).
+constexpr uint32_t kTopNodesMax = 1u << 18;
+
 struct FlatScene {
     std::vector<DNode> nodes;
     std::vector<DTri> tris;
@@ -20,6 +25,7 @@ struct FlatScene {
     std::vector<float> texels;
     std::vector<DLight> lights;
     uint32_t depth = 0;
+    uint32_t top_nodes = 0;   // nodes of the upper levels, stored first (breadth first)
     float sah_cost = 0.0f;
     double build_ms = 0.0;
 };

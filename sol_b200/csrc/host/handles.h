@@ -9,6 +9,7 @@
 
 #include "../../../include/sol_gpu.h"
 #include "../core/layout.h"
+#include "../kernels/kernels.h"
 
 struct SolGpuScene {
     int device = 0;
@@ -25,6 +26,7 @@ struct SolGpuScene {
     sol_b200::DeviceCounters* counters = nullptr;
     unsigned int* fault = nullptr;   // kFault* bits set by the kernels' self-checks
     float* split_scratch = nullptr;  // per-sample colours of split-schedule renders
+    sol_b200::L2Window l2;           // upper BVH levels kept in L2 by the render launches
     float4* adj_texels4 = nullptr;   // interleaved texel gradients of sol_gpu_adjoint
     uint64_t adj_texels4_count = 0;
     size_t split_floats = 0;

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "../core/layout.h"
 #include "../../../include/sol_gpu.h"
 
@@ -26,6 +28,18 @@ constexpr int kTraceBlock = 128;
 /// Largest per-sample colour scratch a split-schedule render may use.
 constexpr size_t kSplitScratchMaxBytes = size_t(256) << 20;
 
+#ifndef SOL_L2_PERSIST
+#define SOL_L2_PERSIST 0   // 1: L2 access-policy window over the upper BVH levels (measured no gain: L2 already keeps them)
+#endif
+
+/// A range of device memory that a launch asks L2 to keep (persisting lines):
+/// the upper BVH levels, stored first in the node array.  bytes == 0: none.
+struct L2Window {
+    const void* base = nullptr;
+    size_t bytes = 0;
+    float hit_ratio = 1.0f;
+};
+
 /// Resident blocks per SM of the megakernel (for sizing its persistent grid).
 int megakernel_blocks_per_sm(bool instrumented);
 
@@ -35,7 +49,7 @@ int megakernel_blocks_per_sm(bool instrumented);
 cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                               uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
                               float* film, DeviceCounters* counters, bool instrumented, int grid,
-                              cudaStream_t stream);
+                              cudaStream_t stream, const L2Window& l2 = {});
 
 /// K1 in the split schedule for small images: every (pixel, sample) is its own
 /// work item; the path colours go to `scratch` (sample_count x 3 planes of
@@ -44,7 +58,7 @@ cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DCon
 cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                                     uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
                                     float* film, float* scratch, DeviceCounters* counters, bool instrumented, int grid,
-                                    cudaStream_t stream);
+                                    cudaStream_t stream, const L2Window& l2 = {});
 
 struct WfView;
 
@@ -57,7 +71,7 @@ int megakernel_views_blocks_per_sm();
 /// are ORed into `*fault`.
 cudaError_t launch_megakernel_views(const WfView* views, uint32_t num_views, uint32_t total_items, uint32_t max_spp,
                                     const SceneView* scenes, const DConfig& cfg, DeviceCounters* counters,
-                                    unsigned int* fault, int grid, cudaStream_t stream);
+                                    unsigned int* fault, int grid, cudaStream_t stream, const L2Window& l2 = {});
 
 /// Sum pass of the split views of launch_megakernel_views (see WfView::split).
 cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, uint64_t total_floats,
@@ -66,5 +80,29 @@ cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, ui
 /// K9: closest-hit or any-hit queries for a batch of rays.
 cudaError_t launch_trace(const SceneView& s, const SolGpuRay* rays, uint32_t count, bool any_hit,
                          SolGpuHit* hits, cudaStream_t stream);
+
+/// Launches `kernel` with an L2 access-policy window (persisting hits on
+/// l2.base .. + l2.bytes, streaming misses) when l2.bytes > 0, otherwise plainly.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_l2(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t stream,
+                      const L2Window& l2, Args&&... args) {
+    cudaLaunchConfig_t c{};
+    c.gridDim = dim3((unsigned)grid);
+    c.blockDim = dim3((unsigned)block);
+    c.dynamicSmemBytes = smem;
+    c.stream = stream;
+    cudaLaunchAttribute attr[1];
+    if (l2.bytes > 0) {
+        attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[0].val.accessPolicyWindow.base_ptr = const_cast<void*>(l2.base);
+        attr[0].val.accessPolicyWindow.num_bytes = l2.bytes;
+        attr[0].val.accessPolicyWindow.hitRatio = l2.hit_ratio;
+        attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        c.attrs = attr;
+        c.numAttrs = 1;
+    }
+    return cudaLaunchKernelEx(&c, kernel, std::forward<Args>(args)...);
+}
 
 }  // namespace sol_b200

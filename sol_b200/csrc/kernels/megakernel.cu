@@ -339,12 +339,12 @@ int megakernel_blocks_per_sm(bool instrumented) {
 cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                               uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
                               float* film, DeviceCounters* counters, bool instrumented, int grid,
-                              cudaStream_t stream) {
+                              cudaStream_t stream, const L2Window& l2) {
     if (instrumented)
-        pt_megakernel<true, false><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, film, counters);
-    else
-        pt_megakernel<false, false><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, film, counters);
-    return cudaGetLastError();
+        return launch_l2(pt_megakernel<true, false>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg, sample_index,
+                         sample_count, width, height, film, counters);
+    return launch_l2(pt_megakernel<false, false>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg, sample_index,
+                     sample_count, width, height, film, counters);
 }
 
 int megakernel_views_blocks_per_sm() {
@@ -355,10 +355,9 @@ int megakernel_views_blocks_per_sm() {
 
 cudaError_t launch_megakernel_views(const WfView* views, uint32_t num_views, uint32_t total_items, uint32_t max_spp,
                                     const SceneView* scenes, const DConfig& cfg, DeviceCounters* counters,
-                                    unsigned int* fault, int grid, cudaStream_t stream) {
-    pt_megakernel_views<false><<<grid, kMegakernelBlock, 0, stream>>>(views, num_views, total_items, max_spp, scenes,
-                                                                       cfg, counters, fault);
-    return cudaGetLastError();
+                                    unsigned int* fault, int grid, cudaStream_t stream, const L2Window& l2) {
+    return launch_l2(pt_megakernel_views<false>, grid, kMegakernelBlock, 0, stream, l2, views, num_views, total_items,
+                     max_spp, scenes, cfg, counters, fault);
 }
 
 cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, uint64_t total_floats,
@@ -372,12 +371,12 @@ cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, ui
 cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                                     uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
                                     float* film, float* scratch, DeviceCounters* counters, bool instrumented, int grid,
-                                    cudaStream_t stream) {
-    if (instrumented)
-        pt_megakernel<true, true><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, scratch, counters);
-    else
-        pt_megakernel<false, true><<<grid, kMegakernelBlock, 0, stream>>>(s, cam, cfg, sample_index, sample_count, width, height, scratch, counters);
-    cudaError_t e = cudaGetLastError();
+                                    cudaStream_t stream, const L2Window& l2) {
+    cudaError_t e = instrumented
+        ? launch_l2(pt_megakernel<true, true>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg, sample_index,
+                    sample_count, width, height, scratch, counters)
+        : launch_l2(pt_megakernel<false, true>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg, sample_index,
+                    sample_count, width, height, scratch, counters);
     if (e != cudaSuccess) return e;
     const size_t plane = (size_t)width * height;
     const int blocks = (int)std::min<size_t>((3 * plane + 255) / 256, 4096);
