@@ -62,6 +62,26 @@ def dist_env():
     return rank, world, local
 
 
+def rank_sample_base(rank: int, spp: int, warmup: int, steps: int) -> int:
+    """First sample index of a rank: every rank renders its own sample range of
+    the frame (warm-up, timed steps and the end-to-end pass, spp samples each),
+    so ranks never render the same path (weak scaling, no collective on the
+    data path; summing the films afterwards would give the frame over all
+    ranks' samples)."""
+    return rank * spp * (warmup + steps + 1)
+
+
+def reduce_max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's time (every rank calls this in the same order)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def load_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -210,7 +230,7 @@ def run_ours(args):
     film = torch.zeros((3, h, w), dtype=torch.float32, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
-    base = rank * spp * (args.warmup + args.steps + 1)
+    base = rank_sample_base(rank, spp, args.warmup, args.steps)
 
     def barrier():
         if world > 1:
@@ -218,11 +238,7 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def reduce_max(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max_over_ranks(x, world)
 
     # Warm-up.
     for i in range(args.warmup):
@@ -274,11 +290,14 @@ def run_ours(args):
     peak, peak_src = load_peaks()
     achieved = alg_bytes / (kernel_s / args.steps) / 1e9
     traffic = None
+    measured = {}
     tfile = ROOT / "profiles" / "megakernel_sphere_field_traffic.txt"
     if tfile.exists() and not args.small:
         for line in tfile.read_text().splitlines():
-            if line.startswith("dram_bytes_per_launch:"):
-                traffic = float(line.split(":", 1)[1])
+            if ":" in line and not line.startswith("#"):
+                key, val = line.split(":", 1)
+                measured[key.strip()] = float(val)
+        traffic = measured.get("dram_bytes_per_launch")
     line = None
     if rank == 0:
         line = {
@@ -291,6 +310,11 @@ def run_ours(args):
             "mrays_per_s": world * rays_per_step * args.steps / kernel_s / 1e6,
             "rays_per_path": rays_per_step / paths,
             "bytes_per_ray": alg_bytes / ist.rays,
+            "ncu_bytes_per_ray": None if not measured else {
+                "dram_read": measured.get("dram_bytes_read", 0.0) / ist.rays,
+                "dram_write": measured.get("dram_bytes_write", 0.0) / ist.rays,
+                "lts": measured.get("lts_bytes", 0.0) / ist.rays,
+                "source": "profiles/megakernel_sphere_field_traffic.txt (one-pass ncu capture of a full launch)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
