@@ -315,6 +315,11 @@ def run_ours(args):
                 "dram_write": measured.get("dram_bytes_write", 0.0) / ist.rays,
                 "lts": measured.get("lts_bytes", 0.0) / ist.rays,
                 "source": "profiles/megakernel_sphere_field_traffic.txt (one-pass ncu capture of a full launch)"},
+            "achieved_gbs": None if not measured else {
+                "dram": (measured.get("dram_bytes_read", 0.0) + measured.get("dram_bytes_write", 0.0))
+                        / (kernel_s / args.steps) / 1e9,
+                "l2": measured.get("lts_bytes", 0.0) / (kernel_s / args.steps) / 1e9,
+                "note": "ncu bytes of one launch over this run's per-launch kernel time"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
