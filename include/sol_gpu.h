@@ -209,6 +209,18 @@ int sol_gpu_device_count(int* count);
  * (src/triangle_mesh.cpp:44-60, include/sol/scene.h:34-48). */
 int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** out);
 
+/* Scene creation flags. */
+#define SOL_GPU_SCENE_GPU_BVH 1u   /* build the BVH on the device (linear BVH, Karras 2012) instead of
+                                      the host's SAH build: much faster for large meshes, a lower-quality
+                                      hierarchy; closest hits at exactly equal distances may resolve to
+                                      another triangle than with the host build.  Ignored when the
+                                      description carries a BVH or has fewer than 2 triangles. */
+
+/* sol_gpu_scene_create with flags (SOL_GPU_SCENE_*); sol_gpu_scene_create is
+ * this with flags = 0.  Fails with SOL_GPU_ERR_UNSUPPORTED when a device-built
+ * hierarchy is deeper than the traversal stack (64). */
+int sol_gpu_scene_create_ex(const SolGpuSceneDesc* desc, int device, uint32_t flags, SolGpuScene** out);
+
 /* sol::PerspectiveCamera's constructor (src/cameras.cpp:5-21): `fov` is the
  * horizontal field of view in degrees, `aspect` = width / height. */
 int sol_gpu_camera_perspective(const float eye[3], const float dir[3], const float up[3], float fov, float aspect,

@@ -23,7 +23,7 @@ BUILD_DIR = PKG / "_build"
 LIB = LIB_DIR / "libsol_gpu.so"
 
 CUDA_SOURCES = ["kernels/megakernel.cu", "kernels/trace.cu", "kernels/wavefront.cu", "kernels/adjoint.cu",
-                "noalloc.cu"]
+                "kernels/lbvh.cu", "noalloc.cu"]
 HOST_SOURCES = ["capi.cpp", "batch.cpp", "job.cpp", "host/flatten.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

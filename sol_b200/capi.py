@@ -25,6 +25,7 @@ ERR_UNSUPPORTED = -7
 ERR_CANCELLED = -8
 SCHEDULE_AUTO, SCHEDULE_PER_PIXEL, SCHEDULE_SPLIT = 0, 1, 2
 BATCH_WAVEFRONT, BATCH_MEGAKERNEL, BATCH_AUTO = 0, 1, 2
+SCENE_GPU_BVH = 1
 
 BSDF_DIFFUSE, BSDF_PHONG, BSDF_MIRROR, BSDF_GLASS, BSDF_INTERP = range(5)
 TEX_CONSTANT, TEX_CONSTANT_COLOR, TEX_IMAGE = range(3)
@@ -123,6 +124,7 @@ SIGNATURES = [
     ("sol_gpu_abi_version", C.c_int, []),
     ("sol_gpu_device_count", C.c_int, [C.POINTER(C.c_int)]),
     ("sol_gpu_scene_create", C.c_int, [C.POINTER(SolGpuSceneDesc), C.c_int, C.POINTER(ScenePtr)]),
+    ("sol_gpu_scene_create_ex", C.c_int, [C.POINTER(SolGpuSceneDesc), C.c_int, C.c_uint32, C.POINTER(ScenePtr)]),
     ("sol_gpu_camera_perspective", C.c_int, [C.c_float * 3, C.c_float * 3, C.c_float * 3, C.c_float, C.c_float,
                                              C.POINTER(SolGpuCamera)]),
     ("sol_gpu_scene_destroy", C.c_int, [ScenePtr]),

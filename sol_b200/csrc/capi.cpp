@@ -12,6 +12,7 @@
 #include "core/layout.h"
 #include "host/flatten.h"
 #include "host/handles.h"
+#include "kernels/lbvh.h"
 #include "kernels/adjoint.h"
 #include "kernels/kernels.h"
 
@@ -160,11 +161,16 @@ int sol_gpu_device_count(int* count) {
 }
 
 int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** out) {
+    return sol_gpu_scene_create_ex(desc, device, 0u, out);
+}
+
+int sol_gpu_scene_create_ex(const SolGpuSceneDesc* desc, int device, uint32_t flags, SolGpuScene** out) {
     if (!desc || !out) return fail(SOL_GPU_ERR_INVALID_ARG, "desc and out must not be NULL");
     *out = nullptr;
+    const bool gpu_bvh = (flags & SOL_GPU_SCENE_GPU_BVH) && desc->num_bvh_nodes == 0 && desc->num_triangles >= 2;
     FlatScene flat;
     std::string err;
-    if (!flatten_scene(*desc, flat, err)) return fail(SOL_GPU_ERR_INVALID_ARG, err);
+    if (!flatten_scene(*desc, flat, err, !gpu_bvh)) return fail(SOL_GPU_ERR_INVALID_ARG, err);
 
     DeviceGuard guard(device);
     if (guard.err != cudaSuccess) return cuda_fail(guard.err, "cudaSetDevice");
@@ -174,9 +180,55 @@ int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** 
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev_start);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev_stop);
-    if (e == cudaSuccess) e = upload(&s->nodes, flat.nodes);
-    if (e == cudaSuccess) e = upload(&s->tris, flat.tris);
-    if (e == cudaSuccess) e = upload(&s->shade, flat.shade);
+    float gpu_build_ms = 0.0f;
+    if (gpu_bvh && e == cudaSuccess) {
+        // Build the hierarchy on the device from the mesh arrays.
+        const uint32_t nv = desc->num_vertices, nt = desc->num_triangles;
+        float *d_v = nullptr, *d_n = nullptr, *d_uv = nullptr;
+        uint32_t* d_i = nullptr;
+        int32_t *d_b = nullptr, *d_l = nullptr;
+        auto up = [&](void** dst, const void* src, size_t bytes) {
+            if (e != cudaSuccess) return;
+            e = cudaMalloc(dst, bytes ? bytes : 1);
+            if (e == cudaSuccess && bytes) e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+        };
+        cudaEvent_t b0, b1;
+        cudaEventCreate(&b0);
+        cudaEventCreate(&b1);
+        cudaEventRecord(b0, s->stream);
+        up(reinterpret_cast<void**>(&d_v), desc->vertices, sizeof(float) * 3 * nv);
+        up(reinterpret_cast<void**>(&d_n), desc->normals, sizeof(float) * 3 * nv);
+        up(reinterpret_cast<void**>(&d_uv), desc->tex_coords, sizeof(float) * 2 * nv);
+        up(reinterpret_cast<void**>(&d_i), desc->indices, sizeof(uint32_t) * 3 * nt);
+        up(reinterpret_cast<void**>(&d_b), desc->tri_bsdf, sizeof(int32_t) * nt);
+        up(reinterpret_cast<void**>(&d_l), desc->tri_light, sizeof(int32_t) * nt);
+        LbvhResult r;
+        if (e == cudaSuccess) e = build_lbvh(d_v, d_i, d_n, d_uv, d_b, d_l, nt, s->stream, &r);
+        cudaEventRecord(b1, s->stream);
+        cudaEventSynchronize(b1);
+        cudaEventElapsedTime(&gpu_build_ms, b0, b1);
+        cudaEventDestroy(b0);
+        cudaEventDestroy(b1);
+        cudaFree(d_v); cudaFree(d_n); cudaFree(d_uv); cudaFree(d_i); cudaFree(d_b); cudaFree(d_l);
+        if (e == cudaSuccess) {
+            s->nodes = r.nodes;
+            s->tris = r.tris;
+            s->shade = r.shade;
+            flat.depth = r.depth;
+            flat.top_nodes = 0;
+            flat.nodes.assign(r.num_nodes, DNode{});   // sizes only: the arrays are already on the device
+            if (r.depth > (uint32_t)kTraversalStack) {
+                release(s);
+                return fail(SOL_GPU_ERR_UNSUPPORTED, "GPU BVH depth " + std::to_string(r.depth) +
+                                                     " exceeds the traversal stack (64); use the host builder");
+            }
+        }
+    }
+    if (!gpu_bvh) {
+        if (e == cudaSuccess) e = upload(&s->nodes, flat.nodes);
+        if (e == cudaSuccess) e = upload(&s->tris, flat.tris);
+        if (e == cudaSuccess) e = upload(&s->shade, flat.shade);
+    }
     if (e == cudaSuccess) e = upload(&s->bsdfs, flat.bsdfs);
     if (e == cudaSuccess) e = upload(&s->textures, flat.textures);
     if (e == cudaSuccess) e = upload(&s->images, flat.images);
@@ -220,16 +272,16 @@ int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** 
     s->view.num_tris = desc->num_triangles;
     s->view.param_offsets = s->param_offsets;
     s->view.num_nodes = (uint32_t)flat.nodes.size();
-    s->view.max_steps = (uint32_t)std::min<uint64_t>(2ull * (flat.nodes.size() + flat.tris.size()) + 16ull, 0xffffffffull);
+    const size_t num_tris = gpu_bvh ? desc->num_triangles : flat.tris.size();
+    s->view.max_steps = (uint32_t)std::min<uint64_t>(2ull * (flat.nodes.size() + num_tris) + 16ull, 0xffffffffull);
     s->view.fault = s->fault;
 
     s->info.num_triangles = desc->num_triangles;
     s->info.num_nodes = (uint32_t)flat.nodes.size();
     s->info.bvh_depth = flat.depth;
     s->info.sah_cost = flat.sah_cost;
-    s->info.device_bytes = flat.nodes.size() * sizeof(DNode) + flat.tris.size() * sizeof(DTri) +
-                           flat.shade.size() * sizeof(DTriShade);
-    s->info.build_ms = (float)flat.build_ms;
+    s->info.device_bytes = flat.nodes.size() * sizeof(DNode) + num_tris * (sizeof(DTri) + sizeof(DTriShade));
+    s->info.build_ms = (float)flat.build_ms + gpu_build_ms;
 #if SOL_L2_PERSIST
     // Keep the upper BVH levels (stored first) in L2: raise this process's
     // persisting-L2 carve-out up to the device maximum if the range needs it,

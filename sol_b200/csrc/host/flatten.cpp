@@ -62,7 +62,7 @@ SolGpuCamera perspective_camera(const float eye[3], const float dir_in[3], const
     return out;
 }
 
-bool flatten_scene(const SolGpuSceneDesc& d, FlatScene& out, std::string& err) {
+bool flatten_scene(const SolGpuSceneDesc& d, FlatScene& out, std::string& err, bool host_bvh) {
     auto t0 = std::chrono::steady_clock::now();
     const uint32_t nt = d.num_triangles, nv = d.num_vertices;
     if (nt > kMaxTriangles) { err = "too many triangles (max 2^28 - 2)"; return false; }
@@ -180,6 +180,11 @@ bool flatten_scene(const SolGpuSceneDesc& d, FlatScene& out, std::string& err) {
             err = "bad light type"; return false;
         }
         out.lights[i] = o;
+    }
+
+    if (!host_bvh) {
+        out.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return true;
     }
 
     // BVH: the caller's, or built here.

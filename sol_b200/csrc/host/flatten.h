@@ -36,7 +36,9 @@ bvh::Bvh build_mesh_bvh(const float* vertices, const uint32_t* indices, size_t n
 
 /// Validates `desc` and produces the device layout. Returns false with a message
 /// in `err` on invalid input.
-bool flatten_scene(const SolGpuSceneDesc& desc, FlatScene& out, std::string& err);
+/// With host_bvh == false the BVH, triangle and shading arrays are left empty
+/// (the caller builds them on the device).
+bool flatten_scene(const SolGpuSceneDesc& desc, FlatScene& out, std::string& err, bool host_bvh = true);
 
 /// PerspectiveCamera's constructor (src/cameras.cpp:5-21).
 SolGpuCamera perspective_camera(const float eye[3], const float dir[3], const float up[3], float fov, float aspect);

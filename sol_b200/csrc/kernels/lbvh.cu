@@ -1,0 +1,313 @@
+// GPU BVH construction (linear BVH): an alternative to the host builder for
+// large meshes, producing the same device layout (64-byte nodes holding both
+// child boxes, triangles in leaf order, leaves of at most 8 triangles).
+//
+// Method: Karras, "Maximizing Parallelism in the Construction of BVHs, Octrees,
+// and k-d Trees" (HPG 2012).  Triangles are sorted by the 30-bit Morton code of
+// their centroid in the scene's centroid box (the triangle index in the low 32
+// bits makes every key unique); the n - 1 internal nodes of the binary radix
+// tree over the sorted keys are then found independently, node i covering a
+// contiguous range of sorted triangles split where the highest differing key
+// bit changes; boxes are merged bottom-up, the second child to arrive at a node
+// computing its box.  Subtrees of at most 8 triangles become leaves, so an
+// internal node is emitted only when it covers more than 8 triangles (always
+// for the root); the others stay unused in the node array.
+//
+// The hierarchy differs from the host builder's (no SAH, no reinsertion), so
+// closest hits at exactly equal distances may resolve to a different triangle;
+// everything else about the render is unchanged.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include "../core/layout.h"
+#include "../core/math.h"
+#include "lbvh.h"
+
+namespace sol_b200 {
+
+namespace {
+
+constexpr int kLbvhLeafMax = 8;
+
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {   // 10 bits -> every third bit of 30
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+/// float -> uint order-preserving key (for min/max reductions with integer atomics).
+__device__ __forceinline__ uint32_t float_key(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+struct TriBox {
+    float lo[3], hi[3];
+};
+
+__global__ void tri_boxes(const float* __restrict__ v, const uint32_t* __restrict__ idx, uint32_t nt,
+                          TriBox* __restrict__ boxes, uint32_t* __restrict__ cbounds) {
+    __shared__ uint32_t s_lo[3], s_hi[3];
+    if (threadIdx.x < 3) { s_lo[threadIdx.x] = 0xffffffffu; s_hi[threadIdx.x] = 0u; }
+    __syncthreads();
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        TriBox b;
+        for (int k = 0; k < 3; ++k) { b.lo[k] = kFloatMax; b.hi[k] = -kFloatMax; }
+        for (int c = 0; c < 3; ++c) {
+            const uint32_t i = idx[3 * t + c];
+            for (int k = 0; k < 3; ++k) {
+                const float x = v[3 * i + k];
+                b.lo[k] = fminf(b.lo[k], x);
+                b.hi[k] = fmaxf(b.hi[k], x);
+            }
+        }
+        boxes[t] = b;
+        for (int k = 0; k < 3; ++k) {
+            const float c = (b.lo[k] + b.hi[k]) * 0.5f;
+            atomicMin(&s_lo[k], float_key(c));
+            atomicMax(&s_hi[k], float_key(c));
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        atomicMin(&cbounds[threadIdx.x], s_lo[threadIdx.x]);
+        atomicMax(&cbounds[3 + threadIdx.x], s_hi[threadIdx.x]);
+    }
+}
+
+__global__ void morton_keys(const TriBox* __restrict__ boxes, uint32_t nt, const uint32_t* __restrict__ cbounds,
+                            unsigned long long* __restrict__ keys) {
+    float lo[3], ext[3];
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = key_float(cbounds[k]);
+        const float e = key_float(cbounds[3 + k]) - lo[k];
+        ext[k] = e > 0.0f ? e : 1.0f;
+    }
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        const TriBox b = boxes[t];
+        uint32_t m = 0;
+        for (int k = 0; k < 3; ++k) {
+            const float c = ((b.lo[k] + b.hi[k]) * 0.5f - lo[k]) / ext[k];
+            const uint32_t q = (uint32_t)fminf(fmaxf(c * 1024.0f, 0.0f), 1023.0f);
+            m |= expand_bits(q) << (2 - k);
+        }
+        keys[t] = ((unsigned long long)m << 32) | t;
+    }
+}
+
+__device__ __forceinline__ int delta(const unsigned long long* keys, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    return __clzll(keys[i] ^ keys[j]);   // keys are unique, so never 64
+}
+
+/// Internal node i of the radix tree: its range [first, last] and children.
+/// child >= 0: internal node; child < 0: leaf ~sorted_index.
+__global__ void radix_tree(const unsigned long long* __restrict__ keys, int n, int2* __restrict__ range,
+                           int2* __restrict__ child, int* __restrict__ parent_internal, int* __restrict__ parent_leaf) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
+        const int d = delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1) > 0 ? 1 : -1;
+        const int dmin = delta(keys, n, i, i - d);
+        int lmax = 2;
+        while (delta(keys, n, i, i + lmax * d) > dmin) lmax *= 2;   // at most ~log2(n) doublings
+        int l = 0;
+        for (int t = lmax / 2; t >= 1; t /= 2)
+            if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+        const int j = i + l * d;
+        const int dnode = delta(keys, n, i, j);
+        int s = 0;
+        int div = 2;
+        for (int t = (l + div - 1) / div; ; ) {
+            if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+            if (t == 1) break;
+            div *= 2;
+            t = (l + div - 1) / div;
+        }
+        const int gamma = i + s * d + min(d, 0);
+        const int first = min(i, j), last = max(i, j);
+        range[i] = make_int2(first, last);
+        const int left = first == gamma ? ~gamma : gamma;
+        const int right = last == gamma + 1 ? ~(gamma + 1) : gamma + 1;
+        child[i] = make_int2(left, right);
+        if (left >= 0) parent_internal[left] = i; else parent_leaf[~left] = i;
+        if (right >= 0) parent_internal[right] = i; else parent_leaf[~right] = i;
+    }
+}
+
+/// A box written by another block: read from L2 (not a possibly stale L1 line).
+__device__ __forceinline__ TriBox load_box_cg(const TriBox* p) {
+    const float* f = reinterpret_cast<const float*>(p);
+    TriBox b;
+    for (int k = 0; k < 3; ++k) { b.lo[k] = __ldcg(f + k); b.hi[k] = __ldcg(f + 3 + k); }
+    return b;
+}
+
+/// Bottom-up boxes: each leaf walks up; the second arrival at a node merges.
+__global__ void merge_boxes(const unsigned long long* __restrict__ keys, const TriBox* __restrict__ tri_boxes_,
+                            int n, const int2* __restrict__ child, const int* __restrict__ parent_internal,
+                            const int* __restrict__ parent_leaf, TriBox* __restrict__ node_boxes,
+                            unsigned int* __restrict__ arrived) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        int node = parent_leaf[j];
+        for (int guard = 0; node >= 0 && guard < 128; ++guard) {
+            __threadfence();
+            if (atomicAdd(&arrived[node], 1u) == 0u) break;   // the sibling is not done yet
+            const int2 c = child[node];
+            TriBox a = c.x >= 0 ? load_box_cg(node_boxes + c.x) : tri_boxes_[(uint32_t)keys[~c.x]];
+            TriBox b = c.y >= 0 ? load_box_cg(node_boxes + c.y) : tri_boxes_[(uint32_t)keys[~c.y]];
+            TriBox m;
+            for (int k = 0; k < 3; ++k) { m.lo[k] = fminf(a.lo[k], b.lo[k]); m.hi[k] = fmaxf(a.hi[k], b.hi[k]); }
+            node_boxes[node] = m;
+            __threadfence();
+            node = node == 0 ? -1 : parent_internal[node];
+        }
+    }
+}
+
+__device__ __forceinline__ int32_t leaf_ref_(uint32_t first, uint32_t count) {
+    return (int32_t)~((first << 3) | (count - 1u));
+}
+
+__device__ __forceinline__ void put_box(DNode& g, int c, const TriBox& b) {
+    float* xy = c == 0 ? g.b0 : g.b1;
+    xy[0] = b.lo[0]; xy[1] = b.hi[0]; xy[2] = b.lo[1]; xy[3] = b.hi[1];
+    g.b2[2 * c + 0] = b.lo[2]; g.b2[2 * c + 1] = b.hi[2];
+}
+
+/// Device nodes: internal node i is emitted when it covers more than 8
+/// triangles (or is the root); a child covering at most 8 becomes a leaf.
+__global__ void emit_nodes(const unsigned long long* __restrict__ keys, const TriBox* __restrict__ tri_boxes_, int n,
+                           const int2* __restrict__ range, const int2* __restrict__ child,
+                           const TriBox* __restrict__ node_boxes, DNode* __restrict__ nodes) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
+        const int2 r = range[i];
+        if (i != 0 && r.y - r.x + 1 <= kLbvhLeafMax) continue;
+        const int2 c = child[i];
+        DNode g{};
+        for (int side = 0; side < 2; ++side) {
+            const int ch = side == 0 ? c.x : c.y;
+            if (ch < 0) {
+                put_box(g, side, tri_boxes_[(uint32_t)keys[~ch]]);
+                g.ref[side] = leaf_ref_((uint32_t)~ch, 1);
+            } else {
+                put_box(g, side, node_boxes[ch]);
+                const int2 cr = range[ch];
+                const int count = cr.y - cr.x + 1;
+                g.ref[side] = count <= kLbvhLeafMax ? leaf_ref_((uint32_t)cr.x, (uint32_t)count) : ch;
+            }
+        }
+        nodes[i] = g;
+    }
+}
+
+/// Depth of the emitted hierarchy (for the traversal stack bound): every
+/// emitted node counts its emitted ancestors.
+__global__ void node_depth(const int2* __restrict__ range, const int* __restrict__ parent_internal, int n,
+                           unsigned int* __restrict__ max_depth) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
+        const int2 r = range[i];
+        if (i != 0 && r.y - r.x + 1 <= kLbvhLeafMax) continue;
+        unsigned int depth = 1;
+        for (int node = i; node != 0 && depth < 1024u; node = parent_internal[node]) ++depth;
+        atomicMax(max_depth, depth + 1u);   // + the leaf level
+    }
+}
+
+/// Triangles and shading records in leaf (sorted) order.
+__global__ void gather_tris(const unsigned long long* __restrict__ keys, uint32_t nt, const float* __restrict__ v,
+                            const float* __restrict__ nrm, const float* __restrict__ uv, const uint32_t* __restrict__ idx,
+                            const int32_t* __restrict__ tri_bsdf, const int32_t* __restrict__ tri_light,
+                            DTri* __restrict__ tris, DTriShade* __restrict__ shade) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nt; j += gridDim.x * blockDim.x) {
+        const uint32_t p = (uint32_t)keys[j];
+        const uint32_t i0 = idx[3 * p], i1 = idx[3 * p + 1], i2 = idx[3 * p + 2];
+        DTri t;
+        for (int k = 0; k < 3; ++k) { t.v0[k] = v[3 * i0 + k]; t.v1[k] = v[3 * i1 + k]; t.v2[k] = v[3 * i2 + k]; }
+        t.prim = p;
+        t.bsdf = tri_bsdf[p];
+        t.light = tri_light[p];
+        tris[j] = t;
+        DTriShade s;
+        for (int k = 0; k < 3; ++k) { s.n0[k] = nrm[3 * i0 + k]; s.n1[k] = nrm[3 * i1 + k]; s.n2[k] = nrm[3 * i2 + k]; }
+        s.uv0x = uv[2 * i0]; s.uv0y = uv[2 * i0 + 1];
+        s.uv1x = uv[2 * i1]; s.uv1y = uv[2 * i1 + 1];
+        s.uv2x = uv[2 * i2]; s.uv2y = uv[2 * i2 + 1];
+        s.pad = 0.0f;
+        shade[j] = s;
+    }
+}
+
+template <typename T>
+cudaError_t alloc(T** p, size_t n) { return cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * (n ? n : 1)); }
+
+}  // namespace
+
+cudaError_t build_lbvh(const float* vertices, const uint32_t* indices, const float* normals, const float* uvs,
+                       const int32_t* tri_bsdf, const int32_t* tri_light, uint32_t num_triangles,
+                       cudaStream_t stream, LbvhResult* out) {
+    const int n = (int)num_triangles;
+    *out = LbvhResult{};
+    if (n < 2) return cudaErrorInvalidValue;   // the caller uses the host builder for tiny meshes
+    TriBox* boxes = nullptr;
+    TriBox* node_boxes = nullptr;
+    unsigned long long *keys = nullptr, *keys_sorted = nullptr;
+    uint32_t* cbounds = nullptr;
+    int2 *range = nullptr, *child = nullptr;
+    int *parent_internal = nullptr, *parent_leaf = nullptr;
+    unsigned int *arrived = nullptr, *depth = nullptr;
+    void* temp = nullptr;
+    size_t temp_bytes = 0;
+    cudaError_t e = alloc(&boxes, n);
+    if (e == cudaSuccess) e = alloc(&node_boxes, n);
+    if (e == cudaSuccess) e = alloc(&keys, n);
+    if (e == cudaSuccess) e = alloc(&keys_sorted, n);
+    if (e == cudaSuccess) e = alloc(&cbounds, 6);
+    if (e == cudaSuccess) e = alloc(&range, n);
+    if (e == cudaSuccess) e = alloc(&child, n);
+    if (e == cudaSuccess) e = alloc(&parent_internal, n);
+    if (e == cudaSuccess) e = alloc(&parent_leaf, n);
+    if (e == cudaSuccess) e = alloc(&arrived, n);
+    if (e == cudaSuccess) e = alloc(&depth, 1);
+    if (e == cudaSuccess) e = alloc(&out->nodes, n - 1);
+    if (e == cudaSuccess) e = alloc(&out->tris, n);
+    if (e == cudaSuccess) e = alloc(&out->shade, n);
+    const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cbounds, init, sizeof(init), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(arrived, 0, sizeof(unsigned int) * n, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(depth, 0, sizeof(unsigned int), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(out->nodes, 0, sizeof(DNode) * (n - 1), stream);
+    const int grid = (int)std::min<int64_t>((n + 255) / 256, 8192);
+    if (e == cudaSuccess) { tri_boxes<<<grid, 256, 0, stream>>>(vertices, indices, num_triangles, boxes, cbounds); e = cudaGetLastError(); }
+    if (e == cudaSuccess) { morton_keys<<<grid, 256, 0, stream>>>(boxes, num_triangles, cbounds, keys); e = cudaGetLastError(); }
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, keys, keys_sorted, n, 0, 64, stream);
+    if (e == cudaSuccess) e = cudaMalloc(&temp, temp_bytes ? temp_bytes : 1);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(temp, temp_bytes, keys, keys_sorted, n, 0, 64, stream);
+    if (e == cudaSuccess) { radix_tree<<<grid, 256, 0, stream>>>(keys_sorted, n, range, child, parent_internal, parent_leaf); e = cudaGetLastError(); }
+    if (e == cudaSuccess) { merge_boxes<<<grid, 256, 0, stream>>>(keys_sorted, boxes, n, child, parent_internal, parent_leaf, node_boxes, arrived); e = cudaGetLastError(); }
+    if (e == cudaSuccess) { emit_nodes<<<grid, 256, 0, stream>>>(keys_sorted, boxes, n, range, child, node_boxes, out->nodes); e = cudaGetLastError(); }
+    if (e == cudaSuccess) { node_depth<<<grid, 256, 0, stream>>>(range, parent_internal, n, depth); e = cudaGetLastError(); }
+    if (e == cudaSuccess) { gather_tris<<<grid, 256, 0, stream>>>(keys_sorted, num_triangles, vertices, normals, uvs, indices, tri_bsdf, tri_light, out->tris, out->shade); e = cudaGetLastError(); }
+    unsigned int d = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&d, depth, sizeof(d), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    cudaFree(boxes); cudaFree(node_boxes); cudaFree(keys); cudaFree(keys_sorted); cudaFree(cbounds);
+    cudaFree(range); cudaFree(child); cudaFree(parent_internal); cudaFree(parent_leaf); cudaFree(arrived);
+    cudaFree(depth); cudaFree(temp);
+    if (e != cudaSuccess) {
+        cudaFree(out->nodes); cudaFree(out->tris); cudaFree(out->shade);
+        *out = LbvhResult{};
+        return e;
+    }
+    out->num_nodes = (uint32_t)(n - 1);
+    out->depth = d;
+    return cudaSuccess;
+}
+
+}  // namespace sol_b200

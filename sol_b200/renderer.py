@@ -63,12 +63,14 @@ class Image:
 class GpuScene:
     """A scene uploaded to one GPU. `bvh` optionally passes a prebuilt BVH (see scene.build_bvh)."""
 
-    def __init__(self, scene: Scene, device: int = 0, bvh=None):
+    def __init__(self, scene: Scene, device: int = 0, bvh=None, gpu_bvh: bool = False):
+        """`gpu_bvh`: build the hierarchy on the device (SOL_GPU_SCENE_GPU_BVH)."""
         self.scene = scene
         self.device = device
         desc = scene.desc(bvh)
         h = capi.ScenePtr()
-        capi.check(capi.lib.sol_gpu_scene_create(desc.ptr, device, C.byref(h)), "sol_gpu_scene_create")
+        flags = capi.SCENE_GPU_BVH if gpu_bvh else 0
+        capi.check(capi.lib.sol_gpu_scene_create_ex(desc.ptr, device, flags, C.byref(h)), "sol_gpu_scene_create_ex")
         self.handle = h
 
     def info(self) -> capi.SolGpuSceneInfo:
