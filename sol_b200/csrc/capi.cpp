@@ -215,6 +215,7 @@ int sol_gpu_scene_create_ex(const SolGpuSceneDesc* desc, int device, uint32_t fl
             s->tris = r.tris;
             s->shade = r.shade;
             flat.depth = r.depth;
+            flat.sah_cost = r.sah_cost;
             flat.top_nodes = 0;
             flat.nodes.assign(r.num_nodes, DNode{});   // sizes only: the arrays are already on the device
             if (r.depth > (uint32_t)kTraversalStack) {

@@ -3,15 +3,18 @@
 // child boxes, triangles in leaf order, leaves of at most 8 triangles).
 //
 // Method: Karras, "Maximizing Parallelism in the Construction of BVHs, Octrees,
-// and k-d Trees" (HPG 2012).  Triangles are sorted by the 30-bit Morton code of
-// their centroid in the scene's centroid box (the triangle index in the low 32
-// bits makes every key unique); the n - 1 internal nodes of the binary radix
-// tree over the sorted keys are then found independently, node i covering a
-// contiguous range of sorted triangles split where the highest differing key
-// bit changes; boxes are merged bottom-up, the second child to arrive at a node
-// computing its box.  Subtrees of at most 8 triangles become leaves, so an
-// internal node is emitted only when it covers more than 8 triangles (always
-// for the root); the others stay unused in the node array.
+// and k-d Trees" (HPG 2012).  Triangles are sorted by the 63-bit Morton code of
+// their centroid in the scene's centroid box (21 bits per axis, so that the
+// triangles of small, dense objects still get distinct codes); equal codes are
+// ordered by triangle index, which the radix tree uses as the tie-break of its
+// prefix lengths.  The n - 1 internal nodes of the binary radix tree over the
+// sorted keys are then found independently, node i covering a contiguous range
+// of sorted triangles split where the highest differing key bit changes; boxes
+// are merged bottom-up, the second child to arrive at a node computing its box
+// and its surface-area-heuristic cost (traversal 1, triangle 1, as the host
+// builder).  A subtree of at most 8 triangles becomes a leaf when that is
+// cheaper than keeping its split; internal nodes inside a leaf, or that became
+// one, stay unused in the node array.
 //
 // The hierarchy differs from the host builder's (no SAH, no reinsertion), so
 // closest hits at exactly equal distances may resolve to a different triangle;
@@ -31,13 +34,18 @@ namespace sol_b200 {
 namespace {
 
 constexpr int kLbvhLeafMax = 8;
+constexpr float kSahTraversal = 1.0f;   // per node, relative to one triangle test
+constexpr float kSahTriangle = 1.0f;
 
-__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {   // 10 bits -> every third bit of 30
-    v = (v * 0x00010001u) & 0xFF0000FFu;
-    v = (v * 0x00000101u) & 0x0F00F00Fu;
-    v = (v * 0x00000011u) & 0xC30C30C3u;
-    v = (v * 0x00000005u) & 0x49249249u;
-    return v;
+/// 21 bits -> every third bit of 63.
+__device__ __forceinline__ unsigned long long expand_bits21(uint32_t v) {
+    unsigned long long x = v & 0x1fffffu;
+    x = (x | x << 32) & 0x001f00000000ffffull;
+    x = (x | x << 16) & 0x001f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
 }
 
 /// float -> uint order-preserving key (for min/max reductions with integer atomics).
@@ -52,6 +60,11 @@ __device__ __forceinline__ float key_float(uint32_t k) {
 struct TriBox {
     float lo[3], hi[3];
 };
+
+__device__ __forceinline__ float half_area(const TriBox& b) {
+    const float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
 
 __global__ void tri_boxes(const float* __restrict__ v, const uint32_t* __restrict__ idx, uint32_t nt,
                           TriBox* __restrict__ boxes, uint32_t* __restrict__ cbounds) {
@@ -84,7 +97,7 @@ __global__ void tri_boxes(const float* __restrict__ v, const uint32_t* __restric
 }
 
 __global__ void morton_keys(const TriBox* __restrict__ boxes, uint32_t nt, const uint32_t* __restrict__ cbounds,
-                            unsigned long long* __restrict__ keys) {
+                            unsigned long long* __restrict__ keys, uint32_t* __restrict__ order) {
     float lo[3], ext[3];
     for (int k = 0; k < 3; ++k) {
         lo[k] = key_float(cbounds[k]);
@@ -93,19 +106,23 @@ __global__ void morton_keys(const TriBox* __restrict__ boxes, uint32_t nt, const
     }
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
         const TriBox b = boxes[t];
-        uint32_t m = 0;
+        unsigned long long m = 0;
         for (int k = 0; k < 3; ++k) {
             const float c = ((b.lo[k] + b.hi[k]) * 0.5f - lo[k]) / ext[k];
-            const uint32_t q = (uint32_t)fminf(fmaxf(c * 1024.0f, 0.0f), 1023.0f);
-            m |= expand_bits(q) << (2 - k);
+            const uint32_t q = (uint32_t)fminf(fmaxf(c * 2097152.0f, 0.0f), 2097151.0f);
+            m |= expand_bits21(q) << (2 - k);
         }
-        keys[t] = ((unsigned long long)m << 32) | t;
+        keys[t] = m;
+        order[t] = t;
     }
 }
 
+/// Common prefix length of sorted keys i and j, extended by the positions'
+/// common prefix when the keys are equal (every key made unique by its index).
 __device__ __forceinline__ int delta(const unsigned long long* keys, int n, int i, int j) {
     if (j < 0 || j >= n) return -1;
-    return __clzll(keys[i] ^ keys[j]);   // keys are unique, so never 64
+    const unsigned long long x = keys[i] ^ keys[j];
+    return x ? __clzll(x) : 64 + __clz((uint32_t)(i ^ j));
 }
 
 /// Internal node i of the radix tree: its range [first, last] and children.
@@ -149,26 +166,55 @@ __device__ __forceinline__ TriBox load_box_cg(const TriBox* p) {
     return b;
 }
 
-/// Bottom-up boxes: each leaf walks up; the second arrival at a node merges.
-__global__ void merge_boxes(const unsigned long long* __restrict__ keys, const TriBox* __restrict__ tri_boxes_,
-                            int n, const int2* __restrict__ child, const int* __restrict__ parent_internal,
-                            const int* __restrict__ parent_leaf, TriBox* __restrict__ node_boxes,
-                            unsigned int* __restrict__ arrived) {
+/// Bottom-up boxes and SAH costs: each leaf walks up; the second arrival at a
+/// node merges its children's boxes and decides whether the node becomes a leaf
+/// (never the root).  cost(node) = min(leaf: count, split: 1 + sum over the
+/// children of area(child) / area(node) * cost(child)); a triangle costs 1.
+__global__ void merge_boxes(const uint32_t* __restrict__ order, const TriBox* __restrict__ tri_boxes_, int n,
+                            const int2* __restrict__ range, const int2* __restrict__ child,
+                            const int* __restrict__ parent_internal, const int* __restrict__ parent_leaf,
+                            TriBox* __restrict__ node_boxes, float* __restrict__ node_cost,
+                            int* __restrict__ collapse, unsigned int* __restrict__ arrived) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         int node = parent_leaf[j];
         for (int guard = 0; node >= 0 && guard < 128; ++guard) {
             __threadfence();
             if (atomicAdd(&arrived[node], 1u) == 0u) break;   // the sibling is not done yet
             const int2 c = child[node];
-            TriBox a = c.x >= 0 ? load_box_cg(node_boxes + c.x) : tri_boxes_[(uint32_t)keys[~c.x]];
-            TriBox b = c.y >= 0 ? load_box_cg(node_boxes + c.y) : tri_boxes_[(uint32_t)keys[~c.y]];
+            const TriBox a = c.x >= 0 ? load_box_cg(node_boxes + c.x) : tri_boxes_[order[~c.x]];
+            const TriBox b = c.y >= 0 ? load_box_cg(node_boxes + c.y) : tri_boxes_[order[~c.y]];
+            const float ca = c.x >= 0 ? __ldcg(node_cost + c.x) : kSahTriangle;
+            const float cb = c.y >= 0 ? __ldcg(node_cost + c.y) : kSahTriangle;
             TriBox m;
             for (int k = 0; k < 3; ++k) { m.lo[k] = fminf(a.lo[k], b.lo[k]); m.hi[k] = fmaxf(a.hi[k], b.hi[k]); }
+            const float area = half_area(m);
+            const float split = area > 0.0f ? kSahTraversal + (half_area(a) * ca + half_area(b) * cb) / area
+                                            : kSahTraversal + ca + cb;
+            const int2 r = range[node];
+            const int count = r.y - r.x + 1;
+            const bool leaf = node != 0 && count <= kLbvhLeafMax && (float)count * kSahTriangle <= split;
             node_boxes[node] = m;
+            node_cost[node] = leaf ? (float)count * kSahTriangle : split;
+            collapse[node] = leaf ? 1 : 0;
             __threadfence();
             node = node == 0 ? -1 : parent_internal[node];
         }
     }
+}
+
+/// Whether internal node i is emitted: the root, or a node that did not become
+/// a leaf and has no ancestor that did (ancestors covering more than 8
+/// triangles never do, so the walk stops there).
+__device__ __forceinline__ bool emitted(int i, const int2* __restrict__ range, const int* __restrict__ collapse,
+                                        const int* __restrict__ parent_internal) {
+    if (i == 0) return true;
+    if (collapse[i]) return false;
+    for (int p = parent_internal[i], guard = 0; p != 0 && guard < 16; p = parent_internal[p], ++guard) {
+        if (collapse[p]) return false;
+        const int2 r = range[p];
+        if (r.y - r.x + 1 > kLbvhLeafMax) break;
+    }
+    return true;
 }
 
 __device__ __forceinline__ int32_t leaf_ref_(uint32_t first, uint32_t count) {
@@ -181,26 +227,26 @@ __device__ __forceinline__ void put_box(DNode& g, int c, const TriBox& b) {
     g.b2[2 * c + 0] = b.lo[2]; g.b2[2 * c + 1] = b.hi[2];
 }
 
-/// Device nodes: internal node i is emitted when it covers more than 8
-/// triangles (or is the root); a child covering at most 8 becomes a leaf.
-__global__ void emit_nodes(const unsigned long long* __restrict__ keys, const TriBox* __restrict__ tri_boxes_, int n,
+/// Device nodes: every emitted internal node; a child that became a leaf is
+/// referenced as one (its sorted triangle range, at most 8).
+__global__ void emit_nodes(const uint32_t* __restrict__ order, const TriBox* __restrict__ tri_boxes_, int n,
                            const int2* __restrict__ range, const int2* __restrict__ child,
+                           const int* __restrict__ collapse, const int* __restrict__ parent_internal,
                            const TriBox* __restrict__ node_boxes, DNode* __restrict__ nodes) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
-        const int2 r = range[i];
-        if (i != 0 && r.y - r.x + 1 <= kLbvhLeafMax) continue;
+        if (!emitted(i, range, collapse, parent_internal)) continue;
         const int2 c = child[i];
         DNode g{};
         for (int side = 0; side < 2; ++side) {
             const int ch = side == 0 ? c.x : c.y;
             if (ch < 0) {
-                put_box(g, side, tri_boxes_[(uint32_t)keys[~ch]]);
+                put_box(g, side, tri_boxes_[order[~ch]]);
                 g.ref[side] = leaf_ref_((uint32_t)~ch, 1);
             } else {
                 put_box(g, side, node_boxes[ch]);
                 const int2 cr = range[ch];
                 const int count = cr.y - cr.x + 1;
-                g.ref[side] = count <= kLbvhLeafMax ? leaf_ref_((uint32_t)cr.x, (uint32_t)count) : ch;
+                g.ref[side] = collapse[ch] ? leaf_ref_((uint32_t)cr.x, (uint32_t)count) : ch;
             }
         }
         nodes[i] = g;
@@ -209,11 +255,10 @@ __global__ void emit_nodes(const unsigned long long* __restrict__ keys, const Tr
 
 /// Depth of the emitted hierarchy (for the traversal stack bound): every
 /// emitted node counts its emitted ancestors.
-__global__ void node_depth(const int2* __restrict__ range, const int* __restrict__ parent_internal, int n,
-                           unsigned int* __restrict__ max_depth) {
+__global__ void node_depth(const int2* __restrict__ range, const int* __restrict__ collapse,
+                           const int* __restrict__ parent_internal, int n, unsigned int* __restrict__ max_depth) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
-        const int2 r = range[i];
-        if (i != 0 && r.y - r.x + 1 <= kLbvhLeafMax) continue;
+        if (!emitted(i, range, collapse, parent_internal)) continue;
         unsigned int depth = 1;
         for (int node = i; node != 0 && depth < 1024u; node = parent_internal[node]) ++depth;
         atomicMax(max_depth, depth + 1u);   // + the leaf level
@@ -221,12 +266,12 @@ __global__ void node_depth(const int2* __restrict__ range, const int* __restrict
 }
 
 /// Triangles and shading records in leaf (sorted) order.
-__global__ void gather_tris(const unsigned long long* __restrict__ keys, uint32_t nt, const float* __restrict__ v,
+__global__ void gather_tris(const uint32_t* __restrict__ order, uint32_t nt, const float* __restrict__ v,
                             const float* __restrict__ nrm, const float* __restrict__ uv, const uint32_t* __restrict__ idx,
                             const int32_t* __restrict__ tri_bsdf, const int32_t* __restrict__ tri_light,
                             DTri* __restrict__ tris, DTriShade* __restrict__ shade) {
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nt; j += gridDim.x * blockDim.x) {
-        const uint32_t p = (uint32_t)keys[j];
+        const uint32_t p = order[j];
         const uint32_t i0 = idx[3 * p], i1 = idx[3 * p + 1], i2 = idx[3 * p + 2];
         DTri t;
         for (int k = 0; k < 3; ++k) { t.v0[k] = v[3 * i0 + k]; t.v1[k] = v[3 * i1 + k]; t.v2[k] = v[3 * i2 + k]; }
@@ -258,6 +303,9 @@ cudaError_t build_lbvh(const float* vertices, const uint32_t* indices, const flo
     TriBox* boxes = nullptr;
     TriBox* node_boxes = nullptr;
     unsigned long long *keys = nullptr, *keys_sorted = nullptr;
+    uint32_t *order = nullptr, *order_sorted = nullptr;
+    float* node_cost = nullptr;
+    int* collapse = nullptr;
     uint32_t* cbounds = nullptr;
     int2 *range = nullptr, *child = nullptr;
     int *parent_internal = nullptr, *parent_leaf = nullptr;
@@ -268,6 +316,10 @@ cudaError_t build_lbvh(const float* vertices, const uint32_t* indices, const flo
     if (e == cudaSuccess) e = alloc(&node_boxes, n);
     if (e == cudaSuccess) e = alloc(&keys, n);
     if (e == cudaSuccess) e = alloc(&keys_sorted, n);
+    if (e == cudaSuccess) e = alloc(&order, n);
+    if (e == cudaSuccess) e = alloc(&order_sorted, n);
+    if (e == cudaSuccess) e = alloc(&node_cost, n);
+    if (e == cudaSuccess) e = alloc(&collapse, n);
     if (e == cudaSuccess) e = alloc(&cbounds, 6);
     if (e == cudaSuccess) e = alloc(&range, n);
     if (e == cudaSuccess) e = alloc(&child, n);
@@ -281,25 +333,28 @@ cudaError_t build_lbvh(const float* vertices, const uint32_t* indices, const flo
     const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
     if (e == cudaSuccess) e = cudaMemcpyAsync(cbounds, init, sizeof(init), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(arrived, 0, sizeof(unsigned int) * n, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(collapse, 0, sizeof(int) * n, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(depth, 0, sizeof(unsigned int), stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(out->nodes, 0, sizeof(DNode) * (n - 1), stream);
     const int grid = (int)std::min<int64_t>((n + 255) / 256, 8192);
     if (e == cudaSuccess) { tri_boxes<<<grid, 256, 0, stream>>>(vertices, indices, num_triangles, boxes, cbounds); e = cudaGetLastError(); }
-    if (e == cudaSuccess) { morton_keys<<<grid, 256, 0, stream>>>(boxes, num_triangles, cbounds, keys); e = cudaGetLastError(); }
-    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(nullptr, temp_bytes, keys, keys_sorted, n, 0, 64, stream);
+    if (e == cudaSuccess) { morton_keys<<<grid, 256, 0, stream>>>(boxes, num_triangles, cbounds, keys, order); e = cudaGetLastError(); }
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys, keys_sorted, order, order_sorted, n, 0, 63, stream);
     if (e == cudaSuccess) e = cudaMalloc(&temp, temp_bytes ? temp_bytes : 1);
-    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(temp, temp_bytes, keys, keys_sorted, n, 0, 64, stream);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, keys_sorted, order, order_sorted, n, 0, 63, stream);
     if (e == cudaSuccess) { radix_tree<<<grid, 256, 0, stream>>>(keys_sorted, n, range, child, parent_internal, parent_leaf); e = cudaGetLastError(); }
-    if (e == cudaSuccess) { merge_boxes<<<grid, 256, 0, stream>>>(keys_sorted, boxes, n, child, parent_internal, parent_leaf, node_boxes, arrived); e = cudaGetLastError(); }
-    if (e == cudaSuccess) { emit_nodes<<<grid, 256, 0, stream>>>(keys_sorted, boxes, n, range, child, node_boxes, out->nodes); e = cudaGetLastError(); }
-    if (e == cudaSuccess) { node_depth<<<grid, 256, 0, stream>>>(range, parent_internal, n, depth); e = cudaGetLastError(); }
-    if (e == cudaSuccess) { gather_tris<<<grid, 256, 0, stream>>>(keys_sorted, num_triangles, vertices, normals, uvs, indices, tri_bsdf, tri_light, out->tris, out->shade); e = cudaGetLastError(); }
+    if (e == cudaSuccess) { merge_boxes<<<grid, 256, 0, stream>>>(order_sorted, boxes, n, range, child, parent_internal, parent_leaf, node_boxes, node_cost, collapse, arrived); e = cudaGetLastError(); }
+    if (e == cudaSuccess) { emit_nodes<<<grid, 256, 0, stream>>>(order_sorted, boxes, n, range, child, collapse, parent_internal, node_boxes, out->nodes); e = cudaGetLastError(); }
+    if (e == cudaSuccess) { node_depth<<<grid, 256, 0, stream>>>(range, collapse, parent_internal, n, depth); e = cudaGetLastError(); }
+    if (e == cudaSuccess) { gather_tris<<<grid, 256, 0, stream>>>(order_sorted, num_triangles, vertices, normals, uvs, indices, tri_bsdf, tri_light, out->tris, out->shade); e = cudaGetLastError(); }
     unsigned int d = 0;
+    float root_cost = 0.0f;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&d, depth, sizeof(d), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&root_cost, node_cost, sizeof(float), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     cudaFree(boxes); cudaFree(node_boxes); cudaFree(keys); cudaFree(keys_sorted); cudaFree(cbounds);
     cudaFree(range); cudaFree(child); cudaFree(parent_internal); cudaFree(parent_leaf); cudaFree(arrived);
-    cudaFree(depth); cudaFree(temp);
+    cudaFree(depth); cudaFree(temp); cudaFree(order); cudaFree(order_sorted); cudaFree(node_cost); cudaFree(collapse);
     if (e != cudaSuccess) {
         cudaFree(out->nodes); cudaFree(out->tris); cudaFree(out->shade);
         *out = LbvhResult{};
@@ -307,6 +362,7 @@ cudaError_t build_lbvh(const float* vertices, const uint32_t* indices, const flo
     }
     out->num_nodes = (uint32_t)(n - 1);
     out->depth = d;
+    out->sah_cost = root_cost;
     return cudaSuccess;
 }
 

@@ -15,6 +15,7 @@ struct LbvhResult {
     DTriShade* shade = nullptr;    // num_triangles, leaf order
     uint32_t num_nodes = 0;
     uint32_t depth = 0;            // node levels including the leaf level
+    float sah_cost = 0.0f;         // SAH cost (traversal 1, triangle 1) normalised by the root's area
 };
 
 /// Builds the hierarchy on the device from device arrays (vertices 3*nv floats,
