@@ -210,9 +210,10 @@ int sol_gpu_device_count(int* count);
 int sol_gpu_scene_create(const SolGpuSceneDesc* desc, int device, SolGpuScene** out);
 
 /* Scene creation flags. */
-#define SOL_GPU_SCENE_GPU_BVH 1u   /* build the BVH on the device (linear BVH, Karras 2012) instead of
-                                      the host's SAH build: much faster for large meshes, a lower-quality
-                                      hierarchy; closest hits at exactly equal distances may resolve to
+#define SOL_GPU_SCENE_GPU_BVH 1u   /* build the BVH on the device (linear BVH, Karras 2012, with treelet
+                                      restructuring, Karras and Aila 2013) instead of the host's SAH
+                                      build: much faster for large meshes, a hierarchy of similar SAH
+                                      cost; closest hits at exactly equal distances may resolve to
                                       another triangle than with the host build.  Ignored when the
                                       description carries a BVH or has fewer than 2 triangles. */
 

@@ -65,7 +65,8 @@ def test_gpu_built_render_matches_oracle(built, kind):
 
 def test_gpu_build_of_a_million_triangles(built):
     """The benchmark scene (1,048,586 triangles): device build in far less time
-    than the host build, a usable depth, and a frame that matches the host-built
+    than the host build, a usable depth, an SAH cost within 10 % of the host
+    build's (treelet restructuring), and a frame that matches the host-built
     scene's on nearly every pixel."""
     import torch
     from sol_b200 import scenes
@@ -76,6 +77,7 @@ def test_gpu_build_of_a_million_triangles(built):
     assert di.num_triangles == hi.num_triangles == scene.num_triangles
     assert 0 < di.bvh_depth <= 64
     assert di.build_ms < hi.build_ms
+    assert 0 < di.sah_cost <= 1.1 * hi.sah_cost
     films = []
     for gs in (host, dev):
         f = torch.zeros((3, 90, 160), device="cuda")
@@ -84,4 +86,5 @@ def test_gpu_build_of_a_million_triangles(built):
         films.append(f.cpu().numpy())
     exact, bad = per_pixel_parity(films[1], films[0])
     assert bad == 0 and exact >= 0.99
-    print(f"host build {hi.build_ms:.0f} ms, device build {di.build_ms:.0f} ms, depth {hi.bvh_depth} / {di.bvh_depth}")
+    print(f"host build {hi.build_ms:.0f} ms, device build {di.build_ms:.0f} ms, depth {hi.bvh_depth} / {di.bvh_depth}, "
+          f"SAH {hi.sah_cost:.3f} / {di.sah_cost:.3f}")
