@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define SOL_GPU_ABI_VERSION 1
+#define SOL_GPU_ABI_VERSION 2
 
 /* Status codes */
 #define SOL_GPU_OK                  0
@@ -167,6 +167,8 @@ typedef struct SolGpuRenderStats {
     uint64_t nodes_visited;  /* BVH nodes fetched (instrumented renders only) */
     uint64_t tris_tested;    /* triangles tested (instrumented renders only) */
     float kernel_ms;         /* device time of the render kernel(s) */
+    uint32_t launches;       /* kernels the render launched (sol_gpu_render_stats; 0 for batches) */
+    uint32_t sample_chunk;   /* samples per chunk of the split schedule (0: per-pixel schedule or a batch) */
 } SolGpuRenderStats;
 
 /* Description of an uploaded scene. */
@@ -261,15 +263,24 @@ int sol_gpu_scene_set_instrumented(SolGpuScene* scene, int instrumented);
 
 /* Render schedules of sol_gpu_render / sol_gpu_render_device.  Both give the
  * same film bits.  PER_PIXEL: one lane renders all samples of a pixel.  SPLIT:
- * every (pixel, sample) is a work item and the samples are summed per pixel in
- * order afterwards (uses scratch memory of 12 bytes per pixel and sample, at
- * most 256 MiB, held by the scene handle; renders through one handle must
- * therefore be ordered, e.g. issued on one stream).  AUTO (the default) picks
- * SPLIT for images with fewer pixels than twice the resident lanes. */
+ * every (pixel, sample) is a work item, a warp taking one sample of an 8x4
+ * pixel tile, and the samples are summed per pixel in order afterwards; it
+ * uses scratch memory of 12 bytes per pixel and sample, at most 2 GiB (renders
+ * needing more run in chunks of samples, with 12 more bytes per pixel for the
+ * running sums), held by the scene handle, so renders through one handle must
+ * be ordered, e.g. issued on one stream.  AUTO (the default) picks SPLIT for
+ * every render of more than one sample (measured faster at every image size),
+ * PER_PIXEL for single samples or when the scratch cannot be allocated. */
 #define SOL_GPU_SCHEDULE_AUTO      0
 #define SOL_GPU_SCHEDULE_PER_PIXEL 1
 #define SOL_GPU_SCHEDULE_SPLIT     2
 int sol_gpu_scene_set_schedule(SolGpuScene* scene, int schedule);
+
+/* Limit on the split schedule's colour scratch for one render through this
+ * handle, in bytes (0: the default, 2 GiB).  A render whose samples need more
+ * runs in chunks of samples that fit; the film bits do not change.  No
+ * counterpart in the reference (SoL renders on the host). */
+int sol_gpu_scene_set_scratch_limit(SolGpuScene* scene, uint64_t bytes);
 
 /* Closest-hit (any_hit == 0) or any-hit (any_hit != 0) queries for a batch of
  * device-resident rays, the device side of TriangleMesh::intersect_closest /

@@ -83,7 +83,8 @@ class SolGpuConfig(C.Structure):
 
 class SolGpuRenderStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("rays", C.c_uint64), ("shadow_rays", C.c_uint64),
-                ("nodes_visited", C.c_uint64), ("tris_tested", C.c_uint64), ("kernel_ms", C.c_float)]
+                ("nodes_visited", C.c_uint64), ("tris_tested", C.c_uint64), ("kernel_ms", C.c_float),
+                ("launches", C.c_uint32), ("sample_chunk", C.c_uint32)]
 
 
 class SolGpuSceneInfo(C.Structure):
@@ -136,6 +137,7 @@ SIGNATURES = [
     ("sol_gpu_render_stats", C.c_int, [ScenePtr, C.POINTER(SolGpuRenderStats)]),
     ("sol_gpu_scene_set_instrumented", C.c_int, [ScenePtr, C.c_int]),
     ("sol_gpu_scene_set_schedule", C.c_int, [ScenePtr, C.c_int]),
+    ("sol_gpu_scene_set_scratch_limit", C.c_int, [ScenePtr, C.c_uint64]),
     ("sol_gpu_trace", C.c_int, [ScenePtr, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]),
     ("sol_gpu_batch_create", C.c_int, [C.POINTER(ScenePtr), C.c_uint32, C.POINTER(SolGpuBatchOptions),
                                        C.POINTER(BatchPtr)]),

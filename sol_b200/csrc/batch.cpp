@@ -151,20 +151,15 @@ int build_graph(SolGpuBatch* b) {
 /// its split views; views beyond it run per pixel.
 constexpr uint64_t kViewsScratchMaxBytes = uint64_t(4) << 30;
 
-/// Builds and uploads the view table.  For the megakernel schedule, views with
-/// fewer pixels than twice the resident lanes are split ((sample, pixel) work
-/// items, colours in scratch), as sol_gpu_render_device's AUTO schedule would
-/// split them; `sum_floats` receives the size of their sum pass.
+/// Builds and uploads the view table.  For the megakernel schedule, views of
+/// more than one sample are split ((sample, pixel) work items, colours in
+/// scratch), as sol_gpu_render_device's AUTO schedule splits them, in view
+/// order while their scratch fits in kViewsScratchMaxBytes; `sum_floats`
+/// receives the size of their sum pass.
 int upload_views(SolGpuBatch* b, const SolGpuView* views, uint32_t n, uint32_t* total_items, uint64_t* pixels,
                  cudaStream_t stream, bool megakernel = false, uint64_t* sum_floats = nullptr) {
     std::vector<WfView> v(n);
     uint64_t items = 0, px = 0;
-    uint64_t lanes = 0;
-    if (megakernel) {
-        const int per_sm = megakernel_views_blocks_per_sm();
-        if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
-        lanes = (uint64_t)per_sm * b->num_sms * kMegakernelBlock;
-    }
     std::vector<uint64_t> scratch_at(n, 0);
     uint64_t scratch_floats = 0, sum_at = 0;
     if (megakernel) {
@@ -172,7 +167,7 @@ int upload_views(SolGpuBatch* b, const SolGpuView* views, uint32_t n, uint32_t* 
             const SolGpuView& s = views[i];
             const uint64_t plane = (uint64_t)s.width * s.height;
             const uint64_t need = 3 * plane * s.sample_count;
-            if (s.sample_count > 1 && plane < 2 * lanes && (scratch_floats + need) * sizeof(float) <= kViewsScratchMaxBytes) {
+            if (s.sample_count > 1 && (scratch_floats + need) * sizeof(float) <= kViewsScratchMaxBytes) {
                 scratch_at[i] = scratch_floats + 1;   // + 1: 0 marks "not split"
                 scratch_floats += need;
             }

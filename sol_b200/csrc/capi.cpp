@@ -112,36 +112,52 @@ int render_into(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConf
     if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
     int grid = per_sm * scene->num_sms;
     const DCamera cam = to_camera(*camera);
-    // Split schedule when the image has fewer than two pixels per resident lane
-    // and its per-sample colours fit in a modest scratch buffer.
-    const uint64_t lanes = (uint64_t)grid * kMegakernelBlock;
+    // Split schedule (one work item per pixel sample, measured faster than the
+    // per-pixel schedule on small and full-size frames alike) for every render
+    // of more than one sample, in chunks of samples whose colours fit in the
+    // scratch limit; the per-pixel schedule for single samples, on request, or
+    // when not even one sample's colours fit.
     const uint64_t pixels = (uint64_t)width * height;
-    const uint64_t items = (uint64_t)((width + 7) / 8) * ((height + 3) / 4) * 32 * sample_count;
-    const uint64_t scratch_floats = 3 * pixels * sample_count;
-    const bool fits = items < 0x80000000ull && scratch_floats * sizeof(float) <= kSplitScratchMaxBytes;
-    if (scene->schedule == SOL_GPU_SCHEDULE_SPLIT && !fits)
-        return fail(SOL_GPU_ERR_UNSUPPORTED, "the split schedule needs more than 256 MiB of scratch for this render");
-    const bool split = scene->schedule == SOL_GPU_SCHEDULE_SPLIT ||
-                       (scene->schedule == SOL_GPU_SCHEDULE_AUTO && sample_count > 1 && pixels < 2 * lanes && fits);
-    if (split && scene->split_floats < scratch_floats) {
+    const uint64_t sample_items = (uint64_t)((width + 7) / 8) * ((height + 3) / 4) * 32;
+    const uint64_t sample_floats = 3 * pixels;
+    const uint64_t limit = scene->scratch_limit ? scene->scratch_limit : (uint64_t)kSplitScratchMaxBytes;
+    const uint64_t chunk = std::min<uint64_t>({(uint64_t)sample_count, limit / (sample_floats * sizeof(float)),
+                                               0x7fffffffull / sample_items});
+    if (scene->schedule == SOL_GPU_SCHEDULE_SPLIT && chunk == 0)
+        return fail(SOL_GPU_ERR_UNSUPPORTED, "the split schedule needs more than " + std::to_string(limit) +
+                                             " bytes of scratch for one sample of this image");
+    bool split = chunk > 0 && (scene->schedule == SOL_GPU_SCHEDULE_SPLIT ||
+                               (scene->schedule == SOL_GPU_SCHEDULE_AUTO && sample_count > 1));
+    const size_t scratch_floats = split ? (size_t)(chunk * sample_floats) : 0;
+    const size_t running_floats = split && chunk < sample_count ? (size_t)sample_floats : 0;
+    if (split && scene->split_floats < scratch_floats + running_floats) {
         cudaFree(scene->split_scratch);
         scene->split_scratch = nullptr;
         scene->split_floats = 0;
-        e = cudaMalloc(reinterpret_cast<void**>(&scene->split_scratch), scratch_floats * sizeof(float));
-        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc split scratch");
-        scene->split_floats = scratch_floats;
+        e = cudaMalloc(reinterpret_cast<void**>(&scene->split_scratch),
+                       (scratch_floats + running_floats) * sizeof(float));
+        if (e == cudaSuccess) {
+            scene->split_floats = scratch_floats + running_floats;
+        } else if (scene->schedule == SOL_GPU_SCHEDULE_AUTO) {
+            cudaGetLastError();   // no room for the scratch: render per pixel instead
+            split = false;
+        } else {
+            return cuda_fail(e, "cudaMalloc split scratch");
+        }
     }
     cudaEventRecord(scene->ev_start, stream);
     if (split)
         e = launch_megakernel_split(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
-                                    scene->split_scratch, scene->counters, scene->instrumented, grid, stream,
-                                    scene->l2);
+                                    scene->split_scratch, running_floats ? scene->split_scratch + scratch_floats : nullptr,
+                                    (uint32_t)chunk, scene->counters, scene->instrumented, grid, stream, scene->l2);
     else
         e = launch_megakernel(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
                               scene->counters, scene->instrumented, grid, stream, scene->l2);
     if (e != cudaSuccess) return cuda_fail(e, "megakernel launch");
     cudaEventRecord(scene->ev_stop, stream);
     scene->rendered = true;
+    scene->last_chunk = split ? (uint32_t)chunk : 0u;
+    scene->last_launches = split ? 2u * (uint32_t)((sample_count + chunk - 1) / chunk) : 1u;
     return SOL_GPU_OK;
 }
 
@@ -347,6 +363,12 @@ int sol_gpu_scene_set_schedule(SolGpuScene* scene, int schedule) {
     return SOL_GPU_OK;
 }
 
+int sol_gpu_scene_set_scratch_limit(SolGpuScene* scene, uint64_t bytes) {
+    if (!scene) return fail(SOL_GPU_ERR_INVALID_ARG, "scene must not be NULL");
+    scene->scratch_limit = bytes;
+    return SOL_GPU_OK;
+}
+
 int sol_gpu_render_device(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConfig* config,
                           uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
                           float* film_device, void* stream) {
@@ -421,6 +443,8 @@ int sol_gpu_render_stats(SolGpuScene* scene, SolGpuRenderStats* out) {
     out->tris_tested = c.tris;
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, scene->ev_start, scene->ev_stop) == cudaSuccess) out->kernel_ms = ms;
+    out->launches = scene->last_launches;
+    out->sample_chunk = scene->last_chunk;
     return check_fault(scene);
 }
 

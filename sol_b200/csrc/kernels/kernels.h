@@ -25,8 +25,12 @@ namespace sol_b200 {
 constexpr int kMegakernelBlock = SOL_MEGAKERNEL_BLOCK;
 constexpr int kMegakernelMinBlocks = SOL_MEGAKERNEL_MIN_BLOCKS;
 constexpr int kTraceBlock = 128;
-/// Largest per-sample colour scratch a split-schedule render may use.
-constexpr size_t kSplitScratchMaxBytes = size_t(256) << 20;
+#ifndef SOL_SPLIT_SCRATCH_MAX_MB
+#define SOL_SPLIT_SCRATCH_MAX_MB 2048
+#endif
+/// Largest per-sample colour scratch a split-schedule render may use (renders
+/// needing more run their samples in chunks that fit).
+constexpr size_t kSplitScratchMaxBytes = size_t(SOL_SPLIT_SCRATCH_MAX_MB) << 20;
 
 #ifndef SOL_L2_PERSIST
 #define SOL_L2_PERSIST 0   // 1: L2 access-policy window over the upper BVH levels (measured no gain: L2 already keeps them)
@@ -51,14 +55,18 @@ cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DCon
                               float* film, DeviceCounters* counters, bool instrumented, int grid,
                               cudaStream_t stream, const L2Window& l2 = {});
 
-/// K1 in the split schedule for small images: every (pixel, sample) is its own
-/// work item; the path colours go to `scratch` (sample_count x 3 planes of
-/// width*height) and are then added into `film` in sample order.  Same result
-/// bits as launch_megakernel.  `counters` must be zeroed before the launch.
+/// K1 in the split schedule: every (pixel, sample) is its own work item, taken
+/// sample-major so that a warp runs one sample of an 8x4 pixel tile.  Samples
+/// run in chunks of `chunk`: the path colours of a chunk go to `scratch` (chunk
+/// x 3 planes of width*height) and are added in sample order to each pixel's
+/// running sum (`running`, 3 planes; unused when one chunk holds every
+/// sample), which goes into `film` after the last chunk.  Same result bits as
+/// launch_megakernel.  `counters` must be zeroed before the call.
 cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                                     uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
-                                    float* film, float* scratch, DeviceCounters* counters, bool instrumented, int grid,
-                                    cudaStream_t stream, const L2Window& l2 = {});
+                                    float* film, float* scratch, float* running, uint32_t chunk,
+                                    DeviceCounters* counters, bool instrumented, int grid, cudaStream_t stream,
+                                    const L2Window& l2 = {});
 
 struct WfView;
 

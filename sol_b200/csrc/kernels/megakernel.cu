@@ -294,15 +294,19 @@ pt_megakernel_views(const WfView* __restrict__ views, uint32_t num_views, uint32
     }
 }
 
-/// Adds each pixel's per-sample colours (scratch: sample_count x 3 planes) into
-/// the film in sample order, starting from 0 as the per-pixel loop does.
+/// Adds each pixel's per-sample colours of one chunk of samples (scratch:
+/// sample_count x 3 planes) in sample order to the pixel's running sum, which
+/// starts from 0 with the first chunk as the per-pixel loop's sum does; after
+/// the last chunk the sum is added into the film.  One chunk is both.
 __global__ void __launch_bounds__(256)
-sum_samples(const float* __restrict__ scratch, uint32_t sample_count, size_t plane, float* __restrict__ film) {
+sum_samples(const float* __restrict__ scratch, uint32_t sample_count, size_t plane, float* __restrict__ running,
+            bool first, bool last, float* __restrict__ film) {
     const size_t n = 3 * plane;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        float sum = 0.0f;
+        float sum = first ? 0.0f : running[i];
         for (uint32_t k = 0; k < sample_count; ++k) sum += scratch[(size_t)k * n + i];
-        film[i] += sum;
+        if (last) film[i] += sum;
+        else running[i] = sum;
     }
 }
 
@@ -370,18 +374,28 @@ cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, ui
 
 cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                                     uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
-                                    float* film, float* scratch, DeviceCounters* counters, bool instrumented, int grid,
-                                    cudaStream_t stream, const L2Window& l2) {
-    cudaError_t e = instrumented
-        ? launch_l2(pt_megakernel<true, true>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg, sample_index,
-                    sample_count, width, height, scratch, counters)
-        : launch_l2(pt_megakernel<false, true>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg, sample_index,
-                    sample_count, width, height, scratch, counters);
-    if (e != cudaSuccess) return e;
+                                    float* film, float* scratch, float* running, uint32_t chunk,
+                                    DeviceCounters* counters, bool instrumented, int grid, cudaStream_t stream,
+                                    const L2Window& l2) {
+    if (chunk == 0 || (chunk < sample_count && running == nullptr)) return cudaErrorInvalidValue;
     const size_t plane = (size_t)width * height;
     const int blocks = (int)std::min<size_t>((3 * plane + 255) / 256, 4096);
-    sum_samples<<<blocks, 256, 0, stream>>>(scratch, sample_count, plane, film);
-    return cudaGetLastError();
+    for (uint32_t c0 = 0; c0 < sample_count; c0 += chunk) {
+        const uint32_t k = std::min(chunk, sample_count - c0);
+        cudaError_t e = cudaSuccess;
+        if (c0 > 0) e = cudaMemsetAsync(&counters->next_item, 0, sizeof(counters->next_item), stream);
+        if (e != cudaSuccess) return e;
+        e = instrumented
+            ? launch_l2(pt_megakernel<true, true>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg,
+                        sample_index + c0, k, width, height, scratch, counters)
+            : launch_l2(pt_megakernel<false, true>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg,
+                        sample_index + c0, k, width, height, scratch, counters);
+        if (e != cudaSuccess) return e;
+        sum_samples<<<blocks, 256, 0, stream>>>(scratch, k, plane, running, c0 == 0, c0 + k == sample_count, film);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace sol_b200

@@ -109,6 +109,10 @@ class GpuScene:
         """capi.SCHEDULE_AUTO / SCHEDULE_PER_PIXEL / SCHEDULE_SPLIT (same film bits)."""
         capi.check(capi.lib.sol_gpu_scene_set_schedule(self.handle, int(schedule)), "sol_gpu_scene_set_schedule")
 
+    def set_scratch_limit(self, nbytes: int) -> None:
+        """Bytes of split-schedule scratch a render may use (0: default); larger renders run in chunks."""
+        capi.check(capi.lib.sol_gpu_scene_set_scratch_limit(self.handle, int(nbytes)), "sol_gpu_scene_set_scratch_limit")
+
     def trace(self, rays_ptr: int, count: int, any_hit: bool, hits_ptr: int, stream: int = 0) -> None:
         """Device-pointer batch query (SolGpuRay in, SolGpuHit out)."""
         capi.check(capi.lib.sol_gpu_trace(self.handle, rays_ptr, count, int(any_hit), hits_ptr, stream), "sol_gpu_trace")

@@ -217,3 +217,30 @@ def test_schedules_agree_bit_for_bit(built, which):
     o = oracle.render(scene, cfg, w, h, spp, sample_index=11, film=np.full((3, h, w), 0.5, np.float32))
     exact, bad = per_pixel_parity(films[capi.SCHEDULE_SPLIT].cpu().numpy(), o)
     assert bad == 0 and exact >= 0.999
+
+
+@pytest.mark.parametrize("samples_per_chunk", [1, 2, 3])
+def test_split_chunks_agree_bit_for_bit(built, samples_per_chunk):
+    """A split render whose scratch limit holds fewer samples than it renders
+    runs in chunks, carrying each pixel's running sum between them: the film is
+    still the per-pixel schedule's, bit for bit."""
+    import torch
+    from sol_b200 import capi, scenes
+    from sol_b200.renderer import GpuPathTracer, GpuScene
+    scene, cfg, w, h, spp = scenes.sphere_field(6, seed=3, bands=17, segments=32), scenes.SPHERES_CONFIG, 100, 60, 7
+    gs = GpuScene(scene)
+    pt = GpuPathTracer(gs, cfg)
+    stream = torch.cuda.current_stream().cuda_stream
+    films = []
+    for sched, limit in ((capi.SCHEDULE_PER_PIXEL, 0), (capi.SCHEDULE_SPLIT, samples_per_chunk * 12 * w * h)):
+        gs.set_schedule(sched)
+        gs.set_scratch_limit(limit)
+        f = torch.full((3, h, w), 0.25, device="cuda")
+        pt.render_device(f.data_ptr(), w, h, 3, spp, stream)
+        torch.cuda.synchronize()
+        assert pt.stats().paths == w * h * spp
+        films.append(f)
+    assert torch.equal(films[0], films[1])
+    gs.set_scratch_limit(12 * w * h - 1)   # not even one sample fits
+    with pytest.raises(capi.SolGpuError):
+        pt.render_device(films[1].data_ptr(), w, h, 3, spp, stream)
