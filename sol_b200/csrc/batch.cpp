@@ -30,6 +30,7 @@ struct SolGpuBatch {
     WfParams* d_params = nullptr;
     WfCounters* d_ctr = nullptr;
     SceneView* d_scenes = nullptr;
+    std::vector<SceneView> h_scenes;   // the same views on the host (kernel-parameter scene tables)
     WfView* d_views = nullptr;
     size_t views_cap = 0;
     AdjView* d_adj_views = nullptr;
@@ -242,7 +243,8 @@ int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* v
         if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
         cudaEventRecord(b->ev_start, stream);
         if (n > 0) {
-            e = launch_megakernel_views(b->d_views, n, total_items, max_spp, b->d_scenes, to_config(*config), b->d_dc,
+            e = launch_megakernel_views(b->d_views, n, total_items, max_spp, b->d_scenes, b->h_scenes.data(),
+                                        (uint32_t)b->h_scenes.size(), to_config(*config), b->d_dc,
                                         b->scenes[0]->fault, per_sm * b->num_sms, stream,
                                         b->scenes.size() == 1 ? b->scenes[0]->l2 : L2Window{});
             if (e == cudaSuccess) e = launch_sum_samples_views(b->d_views, n, sum_floats, stream);
@@ -356,6 +358,7 @@ int sol_gpu_batch_create(SolGpuScene* const* scenes, uint32_t num_scenes, const 
     if (options) b->opts = *options;
     std::vector<SceneView> views(num_scenes);
     for (uint32_t i = 0; i < num_scenes; ++i) views[i] = scenes[i]->view;
+    b->h_scenes = views;
     cudaError_t e = cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_params), sizeof(WfParams));
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_ctr), sizeof(WfCounters));

@@ -15,7 +15,7 @@ namespace sol_b200 {
 #define SOL_MEGAKERNEL_BLOCK 128
 #endif
 #ifndef SOL_MEGAKERNEL_MIN_BLOCKS
-#define SOL_MEGAKERNEL_MIN_BLOCKS 12  // 40 registers: measured fastest despite spills (latency-bound traversal)
+#define SOL_MEGAKERNEL_MIN_BLOCKS 16  // 32 registers, full occupancy: measured fastest despite spills (split schedule)
 #endif
 #ifndef SOL_MEGAKERNEL_SHARED_STACK
 #define SOL_MEGAKERNEL_SHARED_STACK 0   // 1: first traversal-stack entries in shared memory (measured 5% slower)
@@ -70,6 +70,12 @@ cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, cons
 
 struct WfView;
 
+/// Scenes a multi-view megakernel launch takes as a kernel parameter.
+constexpr uint32_t kViewsTableScenes = 32;
+struct SceneTable {
+    SceneView v[kViewsTableScenes];
+};
+
 /// Resident blocks per SM of the multi-view megakernel.
 int megakernel_views_blocks_per_sm();
 
@@ -77,9 +83,13 @@ int megakernel_views_blocks_per_sm();
 /// each view's film receives the bits launch_megakernel would give it.
 /// `counters` must be zeroed before the launch; kernel self-check failures
 /// are ORed into `*fault`.
+/// `scenes` is the device copy of the batch's scene views and `host_scenes`
+/// the same `num_scenes` views on the host: up to kViewsTableScenes of them go
+/// to the kernel by value (SceneTable), more are read from `scenes`.
 cudaError_t launch_megakernel_views(const WfView* views, uint32_t num_views, uint32_t total_items, uint32_t max_spp,
-                                    const SceneView* scenes, const DConfig& cfg, DeviceCounters* counters,
-                                    unsigned int* fault, int grid, cudaStream_t stream, const L2Window& l2 = {});
+                                    const SceneView* scenes, const SceneView* host_scenes, uint32_t num_scenes,
+                                    const DConfig& cfg, DeviceCounters* counters, unsigned int* fault, int grid,
+                                    cudaStream_t stream, const L2Window& l2 = {});
 
 /// Sum pass of the split views of launch_megakernel_views (see WfView::split).
 cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, uint64_t total_floats,

@@ -178,11 +178,15 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
 /// images) have one item per (sample, pixel) as K1's split schedule does, and
 /// sum_samples_views adds their scratch planes afterwards, so every film has
 /// the bits a separate K1 launch gives it.
-template <bool kCount>
+///
+/// With kTable the scenes come in `table`, a kernel parameter in constant
+/// space as K1's scene is, so the traversal reads array pointers and sizes as
+/// constant operands; otherwise from the device array `scenes`.
+template <bool kCount, bool kTable>
 __global__ void __launch_bounds__(kMegakernelBlock, kMegakernelMinBlocks)
 pt_megakernel_views(const WfView* __restrict__ views, uint32_t num_views, uint32_t total, uint32_t max_spp,
-                    const SceneView* __restrict__ scenes, DConfig cfg, DeviceCounters* __restrict__ ctr,
-                    unsigned int* __restrict__ fault) {
+                    const SceneView* __restrict__ scenes, const __grid_constant__ SceneTable table, DConfig cfg,
+                    DeviceCounters* __restrict__ ctr, unsigned int* __restrict__ fault) {
     TraversalCounters tc{0u, 0u};
     uint32_t n_paths = 0, n_rays = 0, n_shadow = 0;
     LocalStack stack;
@@ -190,7 +194,7 @@ pt_megakernel_views(const WfView* __restrict__ views, uint32_t num_views, uint32
     uint32_t px = 0, py = 0, sample = 0, sample_end = 0, vi = 0;
     Rgb pix_sum = rgb(0.0f);
     PathState ps;
-    const SceneView* s = scenes;
+    const SceneView* s = kTable ? &table.v[0] : scenes;
     float light_pick_prob = 1.0f;
     bool done = false;
     // Self-check bound: a lane claims at most every item, each with at most
@@ -251,7 +255,7 @@ pt_megakernel_views(const WfView* __restrict__ views, uint32_t num_views, uint32
                     sample = k;
                     sample_end = W.split ? k + 1u : W.sample_count;
                     pix_sum = rgb(0.0f);
-                    s = scenes + W.scene;
+                    s = kTable ? &table.v[W.scene] : scenes + W.scene;
                     light_pick_prob = 1.0f / (float)s->num_lights;
                 }
             }
@@ -353,15 +357,23 @@ cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DCon
 
 int megakernel_views_blocks_per_sm() {
     int n = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pt_megakernel_views<false>, kMegakernelBlock, 0) == cudaSuccess
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pt_megakernel_views<false, true>, kMegakernelBlock, 0) ==
+                   cudaSuccess
                ? n : -1;
 }
 
 cudaError_t launch_megakernel_views(const WfView* views, uint32_t num_views, uint32_t total_items, uint32_t max_spp,
-                                    const SceneView* scenes, const DConfig& cfg, DeviceCounters* counters,
-                                    unsigned int* fault, int grid, cudaStream_t stream, const L2Window& l2) {
-    return launch_l2(pt_megakernel_views<false>, grid, kMegakernelBlock, 0, stream, l2, views, num_views, total_items,
-                     max_spp, scenes, cfg, counters, fault);
+                                    const SceneView* scenes, const SceneView* host_scenes, uint32_t num_scenes,
+                                    const DConfig& cfg, DeviceCounters* counters, unsigned int* fault, int grid,
+                                    cudaStream_t stream, const L2Window& l2) {
+    SceneTable table{};
+    if (num_scenes <= kViewsTableScenes) {
+        for (uint32_t i = 0; i < num_scenes; ++i) table.v[i] = host_scenes[i];
+        return launch_l2(pt_megakernel_views<false, true>, grid, kMegakernelBlock, 0, stream, l2, views, num_views,
+                         total_items, max_spp, scenes, table, cfg, counters, fault);
+    }
+    return launch_l2(pt_megakernel_views<false, false>, grid, kMegakernelBlock, 0, stream, l2, views, num_views,
+                     total_items, max_spp, scenes, table, cfg, counters, fault);
 }
 
 cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, uint64_t total_floats,
