@@ -108,9 +108,15 @@ int render_into(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConf
     cudaError_t e = cudaMemsetAsync(scene->counters, 0, sizeof(DeviceCounters), stream);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
     SceneView v = scene->view;
-    int per_sm = megakernel_blocks_per_sm(scene->instrumented);
+    // The full-occupancy build for renders of many paths per resident lane,
+    // the 12-block build (fewer spills per path) for smaller ones.
+    const int per_sm_full = megakernel_blocks_per_sm(scene->instrumented, true);
+    if (per_sm_full <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
+    const uint64_t paths = (uint64_t)width * height * sample_count;
+    const bool full = paths >= kMegakernelFullPathsPerLane * (uint64_t)per_sm_full * scene->num_sms * kMegakernelBlock;
+    const int per_sm = full ? per_sm_full : megakernel_blocks_per_sm(scene->instrumented, false);
     if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
-    int grid = per_sm * scene->num_sms;
+    const int grid = per_sm * scene->num_sms;
     const DCamera cam = to_camera(*camera);
     // Split schedule (one work item per pixel sample, measured faster than the
     // per-pixel schedule on small and full-size frames alike) for every render
@@ -149,10 +155,11 @@ int render_into(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConf
     if (split)
         e = launch_megakernel_split(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
                                     scene->split_scratch, running_floats ? scene->split_scratch + scratch_floats : nullptr,
-                                    (uint32_t)chunk, scene->counters, scene->instrumented, grid, stream, scene->l2);
+                                    (uint32_t)chunk, scene->counters, scene->instrumented, full, grid, stream,
+                                    scene->l2);
     else
         e = launch_megakernel(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
-                              scene->counters, scene->instrumented, grid, stream, scene->l2);
+                              scene->counters, scene->instrumented, full, grid, stream, scene->l2);
     if (e != cudaSuccess) return cuda_fail(e, "megakernel launch");
     cudaEventRecord(scene->ev_stop, stream);
     scene->rendered = true;

@@ -17,6 +17,9 @@ namespace sol_b200 {
 #ifndef SOL_MEGAKERNEL_MIN_BLOCKS
 #define SOL_MEGAKERNEL_MIN_BLOCKS 16  // 32 registers, full occupancy: measured fastest despite spills (split schedule)
 #endif
+#ifndef SOL_MEGAKERNEL_SMALL_MIN_BLOCKS
+#define SOL_MEGAKERNEL_SMALL_MIN_BLOCKS 12   // 40 registers: renders of a few paths per lane, where spills cost more
+#endif
 #ifndef SOL_MEGAKERNEL_SHARED_STACK
 #define SOL_MEGAKERNEL_SHARED_STACK 0   // 1: first traversal-stack entries in shared memory (measured 5% slower)
 #endif
@@ -24,6 +27,10 @@ namespace sol_b200 {
 /// register allocation must allow (the compile-time occupancy target).
 constexpr int kMegakernelBlock = SOL_MEGAKERNEL_BLOCK;
 constexpr int kMegakernelMinBlocks = SOL_MEGAKERNEL_MIN_BLOCKS;
+constexpr int kMegakernelSmallMinBlocks = SOL_MEGAKERNEL_SMALL_MIN_BLOCKS;
+/// K1 renders with at least this many paths per resident lane of the
+/// full-occupancy build use it; smaller renders use the 12-block build.
+constexpr uint64_t kMegakernelFullPathsPerLane = 8;
 constexpr int kTraceBlock = 128;
 #ifndef SOL_SPLIT_SCRATCH_MAX_MB
 #define SOL_SPLIT_SCRATCH_MAX_MB 2048
@@ -44,15 +51,17 @@ struct L2Window {
     float hit_ratio = 1.0f;
 };
 
-/// Resident blocks per SM of the megakernel (for sizing its persistent grid).
-int megakernel_blocks_per_sm(bool instrumented);
+/// Resident blocks per SM of the megakernel (for sizing its persistent grid);
+/// `full`: the full-occupancy build (kMegakernelMinBlocks), else the
+/// kMegakernelSmallMinBlocks build.
+int megakernel_blocks_per_sm(bool instrumented, bool full);
 
 /// K1: renders samples [sample_index, sample_index + sample_count) of every
 /// pixel and adds each pixel's sum into `film` (3 planes of width*height).
 /// `counters` must be zeroed before the launch.
 cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                               uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
-                              float* film, DeviceCounters* counters, bool instrumented, int grid,
+                              float* film, DeviceCounters* counters, bool instrumented, bool full, int grid,
                               cudaStream_t stream, const L2Window& l2 = {});
 
 /// K1 in the split schedule: every (pixel, sample) is its own work item, taken
@@ -65,8 +74,8 @@ cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DCon
 cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                                     uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
                                     float* film, float* scratch, float* running, uint32_t chunk,
-                                    DeviceCounters* counters, bool instrumented, int grid, cudaStream_t stream,
-                                    const L2Window& l2 = {});
+                                    DeviceCounters* counters, bool instrumented, bool full, int grid,
+                                    cudaStream_t stream, const L2Window& l2 = {});
 
 struct WfView;
 

@@ -50,8 +50,8 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
     return v;
 }
 
-template <bool kCount, bool kSplit>
-__global__ void __launch_bounds__(kMegakernelBlock, kMegakernelMinBlocks)
+template <bool kCount, bool kSplit, int kMinBlocks>
+__global__ void __launch_bounds__(kMegakernelBlock, kMinBlocks)
 pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint32_t sample_count,
               uint32_t width, uint32_t height, float* __restrict__ film, DeviceCounters* __restrict__ ctr) {
     const uint32_t tiles_x = (width + 7u) / 8u;
@@ -336,23 +336,32 @@ sum_samples_views(const WfView* __restrict__ views, uint32_t num_views, uint64_t
 
 }  // namespace
 
-int megakernel_blocks_per_sm(bool instrumented) {
+namespace {
+
+/// The K1 instantiation for a counting flag, schedule and occupancy target.
+template <bool kSplit>
+auto megakernel_fn(bool instrumented, bool full) {
+    if (instrumented) return full ? pt_megakernel<true, kSplit, kMegakernelMinBlocks>
+                                  : pt_megakernel<true, kSplit, kMegakernelSmallMinBlocks>;
+    return full ? pt_megakernel<false, kSplit, kMegakernelMinBlocks>
+                : pt_megakernel<false, kSplit, kMegakernelSmallMinBlocks>;
+}
+
+}  // namespace
+
+int megakernel_blocks_per_sm(bool instrumented, bool full) {
     int n = 0;
-    cudaError_t e = instrumented
-        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pt_megakernel<true, false>, kMegakernelBlock, 0)
-        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pt_megakernel<false, false>, kMegakernelBlock, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, megakernel_fn<true>(instrumented, full),
+                                                                  kMegakernelBlock, 0);
     return e == cudaSuccess ? n : -1;
 }
 
 cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                               uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
-                              float* film, DeviceCounters* counters, bool instrumented, int grid,
+                              float* film, DeviceCounters* counters, bool instrumented, bool full, int grid,
                               cudaStream_t stream, const L2Window& l2) {
-    if (instrumented)
-        return launch_l2(pt_megakernel<true, false>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg, sample_index,
-                         sample_count, width, height, film, counters);
-    return launch_l2(pt_megakernel<false, false>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg, sample_index,
-                     sample_count, width, height, film, counters);
+    return launch_l2(megakernel_fn<false>(instrumented, full), grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg,
+                     sample_index, sample_count, width, height, film, counters);
 }
 
 int megakernel_views_blocks_per_sm() {
@@ -387,8 +396,8 @@ cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, ui
 cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                                     uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
                                     float* film, float* scratch, float* running, uint32_t chunk,
-                                    DeviceCounters* counters, bool instrumented, int grid, cudaStream_t stream,
-                                    const L2Window& l2) {
+                                    DeviceCounters* counters, bool instrumented, bool full, int grid,
+                                    cudaStream_t stream, const L2Window& l2) {
     if (chunk == 0 || (chunk < sample_count && running == nullptr)) return cudaErrorInvalidValue;
     const size_t plane = (size_t)width * height;
     const int blocks = (int)std::min<size_t>((3 * plane + 255) / 256, 4096);
@@ -397,11 +406,8 @@ cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, cons
         cudaError_t e = cudaSuccess;
         if (c0 > 0) e = cudaMemsetAsync(&counters->next_item, 0, sizeof(counters->next_item), stream);
         if (e != cudaSuccess) return e;
-        e = instrumented
-            ? launch_l2(pt_megakernel<true, true>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg,
-                        sample_index + c0, k, width, height, scratch, counters)
-            : launch_l2(pt_megakernel<false, true>, grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg,
-                        sample_index + c0, k, width, height, scratch, counters);
+        e = launch_l2(megakernel_fn<true>(instrumented, full), grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg,
+                      sample_index + c0, k, width, height, scratch, counters);
         if (e != cudaSuccess) return e;
         sum_samples<<<blocks, 256, 0, stream>>>(scratch, k, plane, running, c0 == 0, c0 + k == sample_count, film);
         e = cudaGetLastError();
