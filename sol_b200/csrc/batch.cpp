@@ -243,8 +243,10 @@ int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* v
         if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
         cudaEventRecord(b->ev_start, stream);
         if (n > 0) {
+            const bool basic = std::all_of(b->scenes.begin(), b->scenes.end(),
+                                           [](const SolGpuScene* s) { return s->basic_shading; });
             e = launch_megakernel_views(b->d_views, n, total_items, max_spp, b->d_scenes, b->h_scenes.data(),
-                                        (uint32_t)b->h_scenes.size(), to_config(*config), b->d_dc,
+                                        (uint32_t)b->h_scenes.size(), basic, to_config(*config), b->d_dc,
                                         b->scenes[0]->fault, per_sm * b->num_sms, stream,
                                         b->scenes.size() == 1 ? b->scenes[0]->l2 : L2Window{});
             if (e == cudaSuccess) e = launch_sum_samples_views(b->d_views, n, sum_floats, stream);

@@ -110,11 +110,12 @@ int render_into(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConf
     SceneView v = scene->view;
     // The full-occupancy build for renders of many paths per resident lane,
     // the 12-block build (fewer spills per path) for smaller ones.
-    const int per_sm_full = megakernel_blocks_per_sm(scene->instrumented, true);
+    const bool basic = scene->basic_shading;
+    const int per_sm_full = megakernel_blocks_per_sm(scene->instrumented, true, basic);
     if (per_sm_full <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
     const uint64_t paths = (uint64_t)width * height * sample_count;
     const bool full = paths >= kMegakernelFullPathsPerLane * (uint64_t)per_sm_full * scene->num_sms * kMegakernelBlock;
-    const int per_sm = full ? per_sm_full : megakernel_blocks_per_sm(scene->instrumented, false);
+    const int per_sm = full ? per_sm_full : megakernel_blocks_per_sm(scene->instrumented, false, basic);
     if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
     const int grid = per_sm * scene->num_sms;
     const DCamera cam = to_camera(*camera);
@@ -155,11 +156,11 @@ int render_into(SolGpuScene* scene, const SolGpuCamera* camera, const SolGpuConf
     if (split)
         e = launch_megakernel_split(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
                                     scene->split_scratch, running_floats ? scene->split_scratch + scratch_floats : nullptr,
-                                    (uint32_t)chunk, scene->counters, scene->instrumented, full, grid, stream,
-                                    scene->l2);
+                                    (uint32_t)chunk, scene->counters, scene->instrumented, full, basic, grid,
+                                    stream, scene->l2);
     else
         e = launch_megakernel(v, cam, to_config(*config), sample_index, sample_count, width, height, film,
-                              scene->counters, scene->instrumented, full, grid, stream, scene->l2);
+                              scene->counters, scene->instrumented, full, basic, grid, stream, scene->l2);
     if (e != cudaSuccess) return cuda_fail(e, "megakernel launch");
     cudaEventRecord(scene->ev_stop, stream);
     scene->rendered = true;
@@ -299,6 +300,10 @@ int sol_gpu_scene_create_ex(const SolGpuSceneDesc* desc, int device, uint32_t fl
     const size_t num_tris = gpu_bvh ? desc->num_triangles : flat.tris.size();
     s->view.max_steps = (uint32_t)std::min<uint64_t>(2ull * (flat.nodes.size() + num_tris) + 16ull, 0xffffffffull);
     s->view.fault = s->fault;
+    s->basic_shading =
+        std::none_of(flat.textures.begin(), flat.textures.end(),
+                     [](const DTexture& t) { return t.kind == SOL_GPU_TEX_IMAGE; }) &&
+        std::none_of(flat.bsdfs.begin(), flat.bsdfs.end(), [](const DBsdf& b) { return b.kind == SOL_GPU_BSDF_INTERP; });
 
     s->info.num_triangles = desc->num_triangles;
     s->info.num_nodes = (uint32_t)flat.nodes.size();

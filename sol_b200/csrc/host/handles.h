@@ -37,6 +37,7 @@ struct SolGpuScene {
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     bool instrumented = false;
     int schedule = SOL_GPU_SCHEDULE_AUTO;
+    bool basic_shading = false;      // no image textures and no Interp BSDFs: K1's basic-shading build applies
     uint64_t scratch_limit = 0;      // split-schedule colour scratch per render (0: kSplitScratchMaxBytes)
     uint32_t last_launches = 0;      // kernels of the last render
     uint32_t last_chunk = 0;         // its samples per split chunk (0: per pixel)

@@ -53,16 +53,17 @@ struct L2Window {
 
 /// Resident blocks per SM of the megakernel (for sizing its persistent grid);
 /// `full`: the full-occupancy build (kMegakernelMinBlocks), else the
-/// kMegakernelSmallMinBlocks build.
-int megakernel_blocks_per_sm(bool instrumented, bool full);
+/// kMegakernelSmallMinBlocks build; `basic`: the build without image textures
+/// and Interp BSDFs, for scenes that have neither (SolGpuScene::basic_shading).
+int megakernel_blocks_per_sm(bool instrumented, bool full, bool basic);
 
 /// K1: renders samples [sample_index, sample_index + sample_count) of every
 /// pixel and adds each pixel's sum into `film` (3 planes of width*height).
 /// `counters` must be zeroed before the launch.
 cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                               uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
-                              float* film, DeviceCounters* counters, bool instrumented, bool full, int grid,
-                              cudaStream_t stream, const L2Window& l2 = {});
+                              float* film, DeviceCounters* counters, bool instrumented, bool full, bool basic,
+                              int grid, cudaStream_t stream, const L2Window& l2 = {});
 
 /// K1 in the split schedule: every (pixel, sample) is its own work item, taken
 /// sample-major so that a warp runs one sample of an 8x4 pixel tile.  Samples
@@ -74,7 +75,7 @@ cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DCon
 cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                                     uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
                                     float* film, float* scratch, float* running, uint32_t chunk,
-                                    DeviceCounters* counters, bool instrumented, bool full, int grid,
+                                    DeviceCounters* counters, bool instrumented, bool full, bool basic, int grid,
                                     cudaStream_t stream, const L2Window& l2 = {});
 
 struct WfView;
@@ -94,11 +95,12 @@ int megakernel_views_blocks_per_sm();
 /// are ORed into `*fault`.
 /// `scenes` is the device copy of the batch's scene views and `host_scenes`
 /// the same `num_scenes` views on the host: up to kViewsTableScenes of them go
-/// to the kernel by value (SceneTable), more are read from `scenes`.
+/// to the kernel by value (SceneTable), more are read from `scenes`.  `basic`:
+/// every scene has basic shading (no image textures, no Interp BSDFs).
 cudaError_t launch_megakernel_views(const WfView* views, uint32_t num_views, uint32_t total_items, uint32_t max_spp,
                                     const SceneView* scenes, const SceneView* host_scenes, uint32_t num_scenes,
-                                    const DConfig& cfg, DeviceCounters* counters, unsigned int* fault, int grid,
-                                    cudaStream_t stream, const L2Window& l2 = {});
+                                    bool basic, const DConfig& cfg, DeviceCounters* counters, unsigned int* fault,
+                                    int grid, cudaStream_t stream, const L2Window& l2 = {});
 
 /// Sum pass of the split views of launch_megakernel_views (see WfView::split).
 cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, uint64_t total_floats,

@@ -50,7 +50,7 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
     return v;
 }
 
-template <bool kCount, bool kSplit, int kMinBlocks>
+template <bool kCount, bool kSplit, int kMinBlocks, bool kBasic>
 __global__ void __launch_bounds__(kMegakernelBlock, kMinBlocks)
 pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint32_t sample_count,
               uint32_t width, uint32_t height, float* __restrict__ film, DeviceCounters* __restrict__ ctr) {
@@ -134,7 +134,7 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
         VertexOut vo;
         vo.has_shadow = false;
         vo.end = slot < 0;
-        if (!vo.end) shade_vertex(s, cfg, light_pick_prob, slot, t, ps, vo);
+        if (!vo.end) shade_vertex<kBasic>(s, cfg, light_pick_prob, slot, t, ps, vo);
 
         // --- shadow ray of this vertex (path_tracer.cpp:72-74) -------------
         if (vo.has_shadow) {
@@ -182,7 +182,7 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
 /// With kTable the scenes come in `table`, a kernel parameter in constant
 /// space as K1's scene is, so the traversal reads array pointers and sizes as
 /// constant operands; otherwise from the device array `scenes`.
-template <bool kCount, bool kTable>
+template <bool kCount, bool kTable, bool kBasic>
 __global__ void __launch_bounds__(kMegakernelBlock, kMegakernelMinBlocks)
 pt_megakernel_views(const WfView* __restrict__ views, uint32_t num_views, uint32_t total, uint32_t max_spp,
                     const SceneView* __restrict__ scenes, const __grid_constant__ SceneTable table, DConfig cfg,
@@ -268,7 +268,7 @@ pt_megakernel_views(const WfView* __restrict__ views, uint32_t num_views, uint32
         VertexOut vo;
         vo.has_shadow = false;
         vo.end = slot < 0;
-        if (!vo.end) shade_vertex(*s, cfg, light_pick_prob, slot, t, ps, vo);
+        if (!vo.end) shade_vertex<kBasic>(*s, cfg, light_pick_prob, slot, t, ps, vo);
         if (vo.has_shadow) {
             float smax = 1.0f - cfg.ray_offset;
             const int occ = traverse<true, kCount>(*s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc, stack);
@@ -338,50 +338,55 @@ sum_samples_views(const WfView* __restrict__ views, uint32_t num_views, uint64_t
 
 namespace {
 
-/// The K1 instantiation for a counting flag, schedule and occupancy target.
+/// The K1 instantiation for a counting flag, schedule, occupancy target and
+/// shading (basic: the scene has no image textures and no Interp BSDFs; the
+/// counting build always has full shading).
 template <bool kSplit>
-auto megakernel_fn(bool instrumented, bool full) {
-    if (instrumented) return full ? pt_megakernel<true, kSplit, kMegakernelMinBlocks>
-                                  : pt_megakernel<true, kSplit, kMegakernelSmallMinBlocks>;
-    return full ? pt_megakernel<false, kSplit, kMegakernelMinBlocks>
-                : pt_megakernel<false, kSplit, kMegakernelSmallMinBlocks>;
+auto megakernel_fn(bool instrumented, bool full, bool basic) {
+    if (instrumented) return full ? pt_megakernel<true, kSplit, kMegakernelMinBlocks, false>
+                                  : pt_megakernel<true, kSplit, kMegakernelSmallMinBlocks, false>;
+    if (basic) return full ? pt_megakernel<false, kSplit, kMegakernelMinBlocks, true>
+                           : pt_megakernel<false, kSplit, kMegakernelSmallMinBlocks, true>;
+    return full ? pt_megakernel<false, kSplit, kMegakernelMinBlocks, false>
+                : pt_megakernel<false, kSplit, kMegakernelSmallMinBlocks, false>;
 }
 
 }  // namespace
 
-int megakernel_blocks_per_sm(bool instrumented, bool full) {
+int megakernel_blocks_per_sm(bool instrumented, bool full, bool basic) {
     int n = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, megakernel_fn<true>(instrumented, full),
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, megakernel_fn<true>(instrumented, full, basic),
                                                                   kMegakernelBlock, 0);
     return e == cudaSuccess ? n : -1;
 }
 
 cudaError_t launch_megakernel(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                               uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
-                              float* film, DeviceCounters* counters, bool instrumented, bool full, int grid,
-                              cudaStream_t stream, const L2Window& l2) {
-    return launch_l2(megakernel_fn<false>(instrumented, full), grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg,
+                              float* film, DeviceCounters* counters, bool instrumented, bool full, bool basic,
+                              int grid, cudaStream_t stream, const L2Window& l2) {
+    return launch_l2(megakernel_fn<false>(instrumented, full, basic), grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg,
                      sample_index, sample_count, width, height, film, counters);
 }
 
 int megakernel_views_blocks_per_sm() {
     int n = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pt_megakernel_views<false, true>, kMegakernelBlock, 0) ==
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pt_megakernel_views<false, true, false>, kMegakernelBlock, 0) ==
                    cudaSuccess
                ? n : -1;
 }
 
 cudaError_t launch_megakernel_views(const WfView* views, uint32_t num_views, uint32_t total_items, uint32_t max_spp,
                                     const SceneView* scenes, const SceneView* host_scenes, uint32_t num_scenes,
-                                    const DConfig& cfg, DeviceCounters* counters, unsigned int* fault, int grid,
-                                    cudaStream_t stream, const L2Window& l2) {
+                                    bool basic, const DConfig& cfg, DeviceCounters* counters, unsigned int* fault,
+                                    int grid, cudaStream_t stream, const L2Window& l2) {
     SceneTable table{};
     if (num_scenes <= kViewsTableScenes) {
         for (uint32_t i = 0; i < num_scenes; ++i) table.v[i] = host_scenes[i];
-        return launch_l2(pt_megakernel_views<false, true>, grid, kMegakernelBlock, 0, stream, l2, views, num_views,
-                         total_items, max_spp, scenes, table, cfg, counters, fault);
+        return launch_l2(basic ? pt_megakernel_views<false, true, true> : pt_megakernel_views<false, true, false>,
+                         grid, kMegakernelBlock, 0, stream, l2, views, num_views, total_items, max_spp, scenes, table,
+                         cfg, counters, fault);
     }
-    return launch_l2(pt_megakernel_views<false, false>, grid, kMegakernelBlock, 0, stream, l2, views, num_views,
+    return launch_l2(pt_megakernel_views<false, false, false>, grid, kMegakernelBlock, 0, stream, l2, views, num_views,
                      total_items, max_spp, scenes, table, cfg, counters, fault);
 }
 
@@ -396,7 +401,7 @@ cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, ui
 cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, const DConfig& cfg,
                                     uint64_t sample_index, uint32_t sample_count, uint32_t width, uint32_t height,
                                     float* film, float* scratch, float* running, uint32_t chunk,
-                                    DeviceCounters* counters, bool instrumented, bool full, int grid,
+                                    DeviceCounters* counters, bool instrumented, bool full, bool basic, int grid,
                                     cudaStream_t stream, const L2Window& l2) {
     if (chunk == 0 || (chunk < sample_count && running == nullptr)) return cudaErrorInvalidValue;
     const size_t plane = (size_t)width * height;
@@ -406,7 +411,7 @@ cudaError_t launch_megakernel_split(const SceneView& s, const DCamera& cam, cons
         cudaError_t e = cudaSuccess;
         if (c0 > 0) e = cudaMemsetAsync(&counters->next_item, 0, sizeof(counters->next_item), stream);
         if (e != cudaSuccess) return e;
-        e = launch_l2(megakernel_fn<true>(instrumented, full), grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg,
+        e = launch_l2(megakernel_fn<true>(instrumented, full, basic), grid, kMegakernelBlock, 0, stream, l2, s, cam, cfg,
                       sample_index + c0, k, width, height, scratch, counters);
         if (e != cudaSuccess) return e;
         sum_samples<<<blocks, 256, 0, stream>>>(scratch, k, plane, running, c0 == 0, c0 + k == sample_count, film);

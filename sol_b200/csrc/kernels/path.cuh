@@ -93,7 +93,7 @@ struct NoRecord {
 /// returned for the caller to trace), Russian roulette (:99-108) and the BSDF
 /// bounce (:110-117), which replaces the state's ray.  `rec` observes the
 /// vertex (see NoRecord).
-template <class Rec>
+template <class Rec, bool kBasic = false>
 __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& cfg, float light_pick_prob,
                                              int slot, float t, PathState& ps, VertexOut& out, Rec& rec) {
     out.end = false;
@@ -108,7 +108,7 @@ __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& 
         const float pdf_prev_area = ps.pdf_prev * dot(out_dir, sf.normal()) / (t * t);
         Rgb le; float pdf_from;
         const DLight light = s.lights[light_id];
-        light_emission(s, light, out_dir, sf.surf, &le, &pdf_from);
+        light_emission<kBasic>(s, light, out_dir, sf.surf, &le, &pdf_from);
         const float mis = ps.pdf_prev != 0.0f ? balance_heuristic(pdf_prev_area, pdf_from * light_pick_prob) : 1.0f;
         ps.color = ps.color + ps.T * le * mis;
         rec.emission(s, light, out_dir, sf, le, mis);
@@ -122,7 +122,7 @@ __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& 
         const DLight light = s.lights[li];
         rec.before_light_sample(light, ps.rng);
         LightSample ls;
-        if (light_sample_area(s, light, ps.rng, sf.point, &ls)) {
+        if (light_sample_area<kBasic>(s, light, ps.rng, sf.point, &ls)) {
             Vec3 in_dir = ls.pos - sf.point;
             float cos_surf = dot(in_dir, sf.normal());
             out.sh_org = sf.point;
@@ -131,11 +131,11 @@ __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& 
             cos_surf = cos_surf * inv_light_dist;
             in_dir = in_dir * inv_light_dist;
             const bool has_area = light.kind != SOL_GPU_LIGHT_POINT;
-            const float pdf_bounce = has_area ? bsdf_pdf(s, bsdf_id, in_dir, sf, out_dir) : 0.0f;
+            const float pdf_bounce = has_area ? bsdf_pdf<kBasic>(s, bsdf_id, in_dir, sf, out_dir) : 0.0f;
             const float pdf_light = ls.pdf_from * light_pick_prob;
             const float geom_term = ls.cos * inv_light_dist * inv_light_dist;
             const float mis = has_area ? balance_heuristic(pdf_light, pdf_bounce * geom_term) : 1.0f;
-            const Rgb f = bsdf_eval(s, bsdf_id, in_dir, sf, out_dir);
+            const Rgb f = bsdf_eval<kBasic>(s, bsdf_id, in_dir, sf, out_dir);
             const float scale = geom_term * cos_surf * mis / pdf_light;
             out.pending = ls.intensity * ps.T * f * scale;
             out.has_shadow = true;
@@ -153,7 +153,7 @@ __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& 
     }
     rec.before_bounce(s, bsdf_id, sf, ps.rng);
     BsdfSample bs;
-    if (!bsdf_sample(s, bsdf_id, ps.rng, sf, out_dir, &bs)) { out.end = true; return; }
+    if (!bsdf_sample<kBasic>(s, bsdf_id, ps.rng, sf, out_dir, &bs)) { out.end = true; return; }
     const float r = bs.cos / (bs.pdf * survival);
     ps.T = ps.T * (bs.color * r);
     ps.org = sf.point;
@@ -163,11 +163,12 @@ __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& 
     rec.bounce(s, bsdf_id, sf, out_dir, bs, r);
 }
 
-/// shade_vertex for the forward render (no observer).
+/// shade_vertex for the forward render (no observer); kBasic as in shading.cuh.
+template <bool kBasic = false>
 __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& cfg, float light_pick_prob,
                                              int slot, float t, PathState& ps, VertexOut& out) {
     NoRecord none;
-    shade_vertex(s, cfg, light_pick_prob, slot, t, ps, out, none);
+    shade_vertex<NoRecord, kBasic>(s, cfg, light_pick_prob, slot, t, ps, out, none);
 }
 
 }  // namespace sol_b200

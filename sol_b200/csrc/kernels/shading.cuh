@@ -85,17 +85,22 @@ __device__ SOL_TEX_FN Rgb image_color(const SceneView& s, const DTexture& t, Vec
 }
 
 /// ColorTexture::sample_color.
+// kBasic: the scene has no image textures and no Interp BSDFs (checked on the
+// host when it is uploaded), so those branches are compiled out of the kernels
+// built for such scenes — a smaller instruction footprint and fewer spills.
+template <bool kBasic = false>
 __device__ __forceinline__ Rgb tex_color(const SceneView& s, int id, Vec2 uv) {
     const DTexture& t = s.textures[id];
-    if (t.kind == SOL_GPU_TEX_IMAGE) return image_color(s, t, uv);
+    if (!kBasic && t.kind == SOL_GPU_TEX_IMAGE) return image_color(s, t, uv);
     return rgb(t.v[0], t.v[1], t.v[2]);
 }
 
 /// Texture::sample: constants return their value, colour textures their luminance.
+template <bool kBasic = false>
 __device__ __forceinline__ float tex_scalar(const SceneView& s, int id, Vec2 uv) {
     const DTexture& t = s.textures[id];
     if (t.kind == SOL_GPU_TEX_CONSTANT) return t.v[0];
-    return luminance(tex_color(s, id, uv));
+    return luminance(tex_color<kBasic>(s, id, uv));
 }
 
 // ---------------------------------------------------------------------------
@@ -134,39 +139,43 @@ __device__ __forceinline__ Rgb phong_eval(Vec3 in_dir, const Surface& sf, Vec3 o
 }
 
 /// Bsdf::eval for the non-interpolating kinds (Mirror and Glass return black).
+template <bool kBasic = false>
 __device__ SOL_SHADE_FN Rgb bsdf_eval_basic(const SceneView& s, const DBsdf& b, Vec3 in_dir, const Surface& sf, Vec3 out_dir) {
     if (b.kind == SOL_GPU_BSDF_DIFFUSE)                       // bsdfs.cpp:35-37
-        return tex_color(s, b.tex[0], sf.uv) * kInvPi;
+        return tex_color<kBasic>(s, b.tex[0], sf.uv) * kInvPi;
     if (b.kind == SOL_GPU_BSDF_PHONG)                         // bsdfs.cpp:68-70
-        return phong_eval(in_dir, sf, out_dir, tex_color(s, b.tex[0], sf.uv), tex_scalar(s, b.tex[1], sf.uv));
+        return phong_eval(in_dir, sf, out_dir, tex_color<kBasic>(s, b.tex[0], sf.uv), tex_scalar<kBasic>(s, b.tex[1], sf.uv));
     return rgb(0.0f);
 }
 
 /// Bsdf::pdf for the non-interpolating kinds (Mirror and Glass return 0).
+template <bool kBasic = false>
 __device__ SOL_SHADE_FN float bsdf_pdf_basic(const SceneView& s, const DBsdf& b, Vec3 in_dir, const Surface& sf, Vec3 out_dir) {
     if (b.kind == SOL_GPU_BSDF_DIFFUSE)                       // bsdfs.cpp:50-52
         return cosine_hemisphere_pdf(positive_dot(in_dir, sf.normal()));
     if (b.kind == SOL_GPU_BSDF_PHONG)                         // bsdfs.cpp:87-89
-        return cosine_power_hemisphere_pdf(tex_scalar(s, b.tex[1], sf.uv), reflect_cosine(in_dir, sf.normal(), out_dir));
+        return cosine_power_hemisphere_pdf(tex_scalar<kBasic>(s, b.tex[1], sf.uv), reflect_cosine(in_dir, sf.normal(), out_dir));
     return 0.0f;
 }
 
+template <bool kBasic = false>
 __device__ __forceinline__ Rgb bsdf_eval(const SceneView& s, int id, Vec3 in_dir, const Surface& sf, Vec3 out_dir) {
     const DBsdf b = s.bsdfs[id];
-    if (b.kind != SOL_GPU_BSDF_INTERP) return bsdf_eval_basic(s, b, in_dir, sf, out_dir);
+    if (kBasic || b.kind != SOL_GPU_BSDF_INTERP) return bsdf_eval_basic<kBasic>(s, b, in_dir, sf, out_dir);
     // bsdfs.cpp:185-190
-    Rgb ea = bsdf_eval_basic(s, s.bsdfs[b.a], in_dir, sf, out_dir);
-    Rgb eb = bsdf_eval_basic(s, s.bsdfs[b.b], in_dir, sf, out_dir);
-    return lerp(ea, eb, tex_scalar(s, b.tex[0], sf.uv));
+    Rgb ea = bsdf_eval_basic<kBasic>(s, s.bsdfs[b.a], in_dir, sf, out_dir);
+    Rgb eb = bsdf_eval_basic<kBasic>(s, s.bsdfs[b.b], in_dir, sf, out_dir);
+    return lerp(ea, eb, tex_scalar<kBasic>(s, b.tex[0], sf.uv));
 }
 
+template <bool kBasic = false>
 __device__ __forceinline__ float bsdf_pdf(const SceneView& s, int id, Vec3 in_dir, const Surface& sf, Vec3 out_dir) {
     const DBsdf b = s.bsdfs[id];
-    if (b.kind != SOL_GPU_BSDF_INTERP) return bsdf_pdf_basic(s, b, in_dir, sf, out_dir);
+    if (kBasic || b.kind != SOL_GPU_BSDF_INTERP) return bsdf_pdf_basic<kBasic>(s, b, in_dir, sf, out_dir);
     // bsdfs.cpp:207-212
-    float pa = bsdf_pdf_basic(s, s.bsdfs[b.a], in_dir, sf, out_dir);
-    float pb = bsdf_pdf_basic(s, s.bsdfs[b.b], in_dir, sf, out_dir);
-    return lerp(pa, pb, tex_scalar(s, b.tex[0], sf.uv));
+    float pa = bsdf_pdf_basic<kBasic>(s, s.bsdfs[b.a], in_dir, sf, out_dir);
+    float pb = bsdf_pdf_basic<kBasic>(s, s.bsdfs[b.b], in_dir, sf, out_dir);
+    return lerp(pa, pb, tex_scalar<kBasic>(s, b.tex[0], sf.uv));
 }
 
 struct BsdfSample {
@@ -183,6 +192,7 @@ __device__ __forceinline__ bool validate(const Surface& sf, const BsdfSample& bs
 }
 
 /// Bsdf::sample for the non-interpolating kinds.
+template <bool kBasic = false>
 __device__ SOL_SHADE_FN bool bsdf_sample_basic(const SceneView& s, const DBsdf& b, Pcg& rng, const Surface& sf,
                                   Vec3 out_dir, BsdfSample* out) {
     if (b.kind == SOL_GPU_BSDF_DIFFUSE) {
@@ -195,13 +205,13 @@ __device__ SOL_SHADE_FN bool bsdf_sample_basic(const SceneView& s, const DBsdf& 
         out->in_dir = ld;
         out->pdf = pdf;
         out->cos = d.z;
-        out->color = tex_color(s, b.tex[0], sf.uv) * kInvPi;
+        out->color = tex_color<kBasic>(s, b.tex[0], sf.uv) * kInvPi;
         return validate(sf, *out, false);
     }
     if (b.kind == SOL_GPU_BSDF_PHONG) {
         // bsdfs.cpp:72-85
-        Rgb ks = tex_color(s, b.tex[0], sf.uv);
-        float ns = tex_scalar(s, b.tex[1], sf.uv);
+        Rgb ks = tex_color<kBasic>(s, b.tex[0], sf.uv);
+        float ns = tex_scalar<kBasic>(s, b.tex[1], sf.uv);
         Mat3 basis = ortho_basis(reflect(-out_dir, sf.normal()));
         float v = rng.next_float();
         float u = rng.next_float();
@@ -219,12 +229,12 @@ __device__ SOL_SHADE_FN bool bsdf_sample_basic(const SceneView& s, const DBsdf& 
         out->in_dir = reflect(-out_dir, sf.normal());
         out->pdf = 1.0f;
         out->cos = 1.0f;
-        out->color = tex_color(s, b.tex[0], sf.uv);
+        out->color = tex_color<kBasic>(s, b.tex[0], sf.uv);
         return validate(sf, *out, false);
     }
     if (b.kind == SOL_GPU_BSDF_GLASS) {
         // bsdfs.cpp:138-165
-        float eta = tex_scalar(s, b.tex[2], sf.uv);
+        float eta = tex_scalar<kBasic>(s, b.tex[2], sf.uv);
         eta = sf.front ? eta : 1.0f / eta;
         float cos_i = dot(out_dir, sf.normal());
         float cos2_t = 1.0f - eta * eta * (1.0f - cos_i * cos_i);
@@ -234,31 +244,32 @@ __device__ SOL_SHADE_FN bool bsdf_sample_basic(const SceneView& s, const DBsdf& 
                 out->in_dir = (eta * cos_i - cos_t) * sf.normal() - eta * out_dir;
                 out->pdf = 1.0f;
                 out->cos = 1.0f;
-                out->color = tex_color(s, b.tex[1], sf.uv) * 1.0f;
+                out->color = tex_color<kBasic>(s, b.tex[1], sf.uv) * 1.0f;
                 return validate(sf, *out, true);
             }
         }
         out->in_dir = reflect(-out_dir, sf.normal());
         out->pdf = 1.0f;
         out->cos = 1.0f;
-        out->color = tex_color(s, b.tex[0], sf.uv);
+        out->color = tex_color<kBasic>(s, b.tex[0], sf.uv);
         return validate(sf, *out, false);
     }
     return false;
 }
 
 /// Bsdf::sample, including InterpBsdf (bsdfs.cpp:192-205).
+template <bool kBasic = false>
 __device__ inline bool bsdf_sample(const SceneView& s, int id, Pcg& rng, const Surface& sf, Vec3 out_dir, BsdfSample* out) {
     const DBsdf b = s.bsdfs[id];
-    if (b.kind != SOL_GPU_BSDF_INTERP) return bsdf_sample_basic(s, b, rng, sf, out_dir, out);
-    float k = tex_scalar(s, b.tex[0], sf.uv);
+    if (kBasic || b.kind != SOL_GPU_BSDF_INTERP) return bsdf_sample_basic<kBasic>(s, b, rng, sf, out_dir, out);
+    float k = tex_scalar<kBasic>(s, b.tex[0], sf.uv);
     int target = b.b, other = b.a;
     if (rng.next_float() > k) { int t = target; target = other; other = t; k = 1.0f - k; }
     const DBsdf bt = s.bsdfs[target];
-    if (!bsdf_sample_basic(s, bt, rng, sf, out_dir, out)) return false;
+    if (!bsdf_sample_basic<kBasic>(s, bt, rng, sf, out_dir, out)) return false;
     const DBsdf bo = s.bsdfs[other];
-    out->pdf = lerp(bsdf_pdf_basic(s, bo, out->in_dir, sf, out_dir), out->pdf, k);
-    out->color = lerp(bsdf_eval_basic(s, bo, out->in_dir, sf, out_dir), out->color, k);
+    out->pdf = lerp(bsdf_pdf_basic<kBasic>(s, bo, out->in_dir, sf, out_dir), out->pdf, k);
+    out->color = lerp(bsdf_eval_basic<kBasic>(s, bo, out->in_dir, sf, out_dir), out->color, k);
     return true;
 }
 
@@ -277,6 +288,7 @@ __device__ __forceinline__ Vec3 ld3(const float* p) { return vec3(p[0], p[1], p[
 
 /// Light::sample_area for the three light kinds (lights.cpp:15-24, 64-77;
 /// shapes.cpp:13-16, 20-25, 33-37).
+template <bool kBasic = false>
 __device__ SOL_SHADE_FN bool light_sample_area(const SceneView& s, const DLight& l, Pcg& rng, Vec3 from, LightSample* out) {
     if (l.kind == SOL_GPU_LIGHT_POINT) {
         out->pos = ld3(l.v0);
@@ -303,7 +315,7 @@ __device__ SOL_SHADE_FN bool light_sample_area(const SceneView& s, const DLight&
     float c = positive_dot(dir, n);
     if (!(c > 0.0f)) return false;
     out->pos = pos;
-    out->intensity = tex_color(s, l.tex, vec2(u, v));
+    out->intensity = tex_color<kBasic>(s, l.tex, vec2(u, v));
     out->pdf_from = l.inv_area;
     out->cos = c;
     return true;
@@ -311,6 +323,7 @@ __device__ SOL_SHADE_FN bool light_sample_area(const SceneView& s, const DLight&
 
 /// Light::emission at a hit point seen along `dir` (pointing away from the
 /// light), lights.cpp:38-40, 94-106.  Returns the intensity and pdf_from.
+template <bool kBasic = false>
 __device__ SOL_SHADE_FN void light_emission(const SceneView& s, const DLight& l, Vec3 dir, Vec2 uv, Rgb* intensity, float* pdf_from) {
     if (l.kind == SOL_GPU_LIGHT_POINT) { *intensity = rgb(0.0f); *pdf_from = 1.0f; return; }
     Vec3 n;
@@ -322,7 +335,7 @@ __device__ SOL_SHADE_FN void light_emission(const SceneView& s, const DLight& l,
     }
     float c = dot(dir, n);
     if (c <= 0.0f) { *intensity = rgb(0.0f); *pdf_from = 1.0f; return; }
-    *intensity = tex_color(s, l.tex, uv);
+    *intensity = tex_color<kBasic>(s, l.tex, uv);
     *pdf_from = l.inv_area;
 }
 
