@@ -244,3 +244,28 @@ def test_split_chunks_agree_bit_for_bit(built, samples_per_chunk):
     gs.set_scratch_limit(12 * w * h - 1)   # not even one sample fits
     with pytest.raises(capi.SolGpuError):
         pt.render_device(films[1].data_ptr(), w, h, 3, spp, stream)
+
+
+@pytest.mark.parametrize("w,h,spp", [(160, 90, 5), (640, 360, 16)])
+def test_basic_shading_build_matches_full(built, w, h, spp):
+    """A scene without image textures and Interp BSDFs renders with the kernels
+    built without those branches; the same scene carrying an image texture that
+    no BSDF uses takes the full build.  Both films must agree bit for bit (the
+    larger frame takes the full-occupancy kernels, the smaller the 12-block ones)."""
+    import dataclasses
+    import torch
+    from sol_b200 import capi, scenes
+    from sol_b200.scene import Texture
+    from sol_b200.renderer import GpuPathTracer, GpuScene
+    basic = scenes.sphere_field(6, seed=3, bands=17, segments=32)
+    full = dataclasses.replace(basic, textures=list(basic.textures) + [Texture(capi.TEX_IMAGE, image=0)],
+                               images=[scenes.noise_texture(8, 5)])
+    stream = torch.cuda.current_stream().cuda_stream
+    films = []
+    for scene in (basic, full):
+        f = torch.zeros((3, h, w), device="cuda")
+        GpuPathTracer(GpuScene(scene), scenes.SPHERES_CONFIG).render_device(f.data_ptr(), w, h, 7, spp, stream)
+        torch.cuda.synchronize()
+        films.append(f)
+    assert float(films[0].abs().sum()) > 0
+    assert torch.equal(films[0], films[1])
