@@ -212,7 +212,7 @@ def run_views(args, ClockSampler, load_peaks):
         equal_rmse={"films_bit_identical": identical, "reference": f"{gt_spp}-spp megakernel render per view",
                     "rmse_plain_mean": float(np.mean(rmse_a)), "rmse_batched_mean": float(np.mean(rmse_b))},
         roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                  "traffic": None, "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)",
+                  "traffic": None, "peak_source": src,
                   "algorithmic_bytes_per_launch": alg},
         e2e={"value": paths * args.steps / e2e_s / 1e6, "unit": METRIC,
              "h2d_bytes_per_step": len(views) * ctypes.sizeof(capi.SolGpuView) + ctypes.sizeof(capi.SolGpuConfig),
