@@ -237,8 +237,14 @@ pt_megakernel_views(const WfView* __restrict__ views, uint32_t num_views, uint32
                 }
                 const uint32_t item = claim_items(&ctr->next_item);
                 if (item >= total) { done = true; break; }
-                uint32_t lo = 0, hi = num_views;
-                while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (views[mid].item_begin <= item) lo = mid; else hi = mid; }
+                // Consecutive claims almost always stay in the lane's current view:
+                // check it before searching the table.
+                uint32_t lo = vi;
+                if (!(views[vi].item_begin <= item && (vi + 1u == num_views || item < views[vi + 1u].item_begin))) {
+                    lo = 0;
+                    uint32_t hi = num_views;
+                    while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (views[mid].item_begin <= item) lo = mid; else hi = mid; }
+                }
                 const WfView& W = views[lo];
                 uint32_t local = item - W.item_begin, k = 0;
                 if (W.split) {
