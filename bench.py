@@ -36,7 +36,7 @@ WORKLOAD = {"workload": "one frame per render call, sphere field (64 displaced U
             "triangles": 1048586, "width": 1920, "height": 1080, "spp": 64, "max_path_len": 8,
             "l2": "flushed between steps (256 MiB write)"}
 METRIC = "Mpaths/s"
-BASELINE_VALUE = None   # no published number exists for this metric
+PUBLISHED_VALUE = None   # no published number exists for this metric
 
 
 def parse():
@@ -307,7 +307,7 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * kernel_s / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None if BASELINE_VALUE is None else value / BASELINE_VALUE,
+            "scaling": "weak", "vs_baseline": None if PUBLISHED_VALUE is None else value / PUBLISHED_VALUE,
             "dtype": "f32", "data": "synthetic (seeded procedural scene)",
             "config": dict(WORKLOAD, parallelism=f"{world} GPU(s), one 64-sample range per rank",
                            small=bool(args.small)),
