@@ -144,6 +144,11 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def workload_config(small: bool) -> dict:
+    """The frame workload's `config` (identical in both arms)."""
+    return dict(WORKLOAD, small=True, width=480, height=270, spp=8) if small else dict(WORKLOAD)
+
+
 def make_workload(small: bool):
     from sol_b200 import scenes
     scene = scenes.sphere_field(64, seed=1)
@@ -151,63 +156,76 @@ def make_workload(small: bool):
     return scene, scenes.SPHERES_CONFIG, w, h, spp
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (first /proc/cpuinfo entry)."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_renderer(scene, threads: int):
+    """SoL's own path tracer (oracle/_ref, which links nothing of this
+    library) on `threads` host threads, or the oracle restatement where SoL's
+    sources were not built; returns (kind, run(sample_index, spp, w, h, cfg) ->
+    seconds of the render call alone)."""
+    import oracle
+    if oracle.ref_available():
+        ref = oracle.RefScene(scene)
+
+        def run(index, spp, w, h, cfg):
+            _, ms = ref.render(cfg, w, h, spp, sample_index=index, threads=threads)
+            return ms / 1000.0
+        return "reference", run
+
+    def run_port(index, spp, w, h, cfg):
+        t = time.perf_counter()
+        oracle.render(scene, cfg, w, h, spp, sample_index=index, threads=threads)
+        return time.perf_counter() - t
+    return "port", run_port
+
+
 def cpu_reference_mpaths(scene, cfg, w, h, target_s: float = 12.0, max_spp: int = 64):
     """SoL's own path tracer on all host threads over whole frames; 1 spp first,
     then enough samples for about `target_s` seconds (paths are independent)."""
-    import oracle
     threads = os.cpu_count() or 1
-    if oracle.ref_available():
-        ref = oracle.RefScene(scene)
-        kind = "reference"
-
-        def run(index, spp):
-            _, ms = ref.render(cfg, w, h, spp, sample_index=index, threads=threads)
-            return ms / 1000.0
-    else:
-        kind = "port"
-
-        def run(index, spp):
-            t = time.perf_counter()
-            oracle.render(scene, cfg, w, h, spp, sample_index=index, threads=threads)
-            return time.perf_counter() - t
-    t1 = run(0, 1)
+    kind, run = cpu_renderer(scene, threads)
+    t1 = run(0, 1, w, h, cfg)
     spp = int(min(max_spp, max(1, math.floor(target_s / max(t1, 1e-3)))))
-    t = run(1, spp) if spp > 1 else t1
+    t = run(1, spp, w, h, cfg) if spp > 1 else t1
     paths = w * h * spp
-    return {"value": paths / t / 1e6, "unit": METRIC, "cores": threads, "kind": kind,
+    return {"value": paths / t / 1e6, "unit": METRIC, "cores": threads, "cpu_model": cpu_model(), "kind": kind,
             "sample": f"{spp} spp of the full {w}x{h} frame ({paths} paths) on {threads} threads, "
                       f"{t:.2f} s; BVH build excluded (test/driver.cpp:232 starts the clock after scene load)"}
 
 
 def run_reference(args):
+    """SoL's CPU PathTracer on the same frame: every step renders all spp
+    samples of every pixel in one Renderer::render call (the work of one step
+    of this library's arm), timed around the call as test/driver.cpp:232-238
+    times a render."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    scene, cfg, w, h, _ = make_workload(args.small)
-    import oracle
+    scene, cfg, w, h, spp = make_workload(args.small)
     threads = os.cpu_count() or 1
-    kind = "reference" if oracle.ref_available() else "port"
-    ref = oracle.RefScene(scene) if kind == "reference" else None
-
-    def step(index, spp=1):
-        if ref is not None:
-            _, ms = ref.render(cfg, w, h, spp, sample_index=index, threads=threads)
-            return ms / 1000.0
-        t = time.perf_counter()
-        oracle.render(scene, cfg, w, h, spp, sample_index=index, threads=threads)
-        return time.perf_counter() - t
+    kind, run = cpu_renderer(scene, threads)
     for i in range(args.warmup):
-        step(i)
-    times = [step(args.warmup + i) for i in range(args.steps)]
+        run(i * spp, spp, w, h, cfg)
+    times = [run((args.warmup + i) * spp, spp, w, h, cfg) for i in range(args.steps)]
     total = sum(times)
-    paths = w * h * args.steps
+    paths = w * h * spp * args.steps
     value = paths / total / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(WORKLOAD, step="1 spp of the full frame per step (bounded CPU sample)"),
-            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": kind,
-                             "sample": f"1 spp of the full {w}x{h} frame per step, {args.steps} steps"},
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scene)", "config": workload_config(args.small),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "cpu_model": cpu_model(), "kind": kind,
+                             "sample": f"{spp} spp of the full {w}x{h} frame per step (one render call), "
+                                       f"{args.steps} steps on {threads} threads"},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -309,8 +327,8 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": 1000.0 * kernel_s / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None if PUBLISHED_VALUE is None else value / PUBLISHED_VALUE,
             "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": dict(WORKLOAD, parallelism=f"{world} GPU(s), one 64-sample range per rank",
-                           small=bool(args.small)),
+            "config": workload_config(args.small),
+            "parallelism": f"{world} GPU(s), one {spp}-sample range per rank",
             "mrays_per_s": world * rays_per_step * args.steps / kernel_s / 1e6,
             "rays_per_path": rays_per_step / paths,
             "bytes_per_ray": alg_bytes / ist.rays,

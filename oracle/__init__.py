@@ -4,7 +4,10 @@ Two checkers, both over the flat scene of include/sol_gpu.h:
   * liboracle.so (oracle/_build/): pt_oracle.cpp, a C++ restatement of SoL's
     path tracer (src/algorithms/path_tracer.cpp and the classes it calls);
   * libsol_ref.so (oracle/_ref/): SoL's own sources compiled against the
-    clean-room proto/par/bvh shims (oracle/Makefile), driven by ref_harness.cpp.
+    clean-room proto/par/bvh shims (oracle/Makefile), driven by ref_harness.cpp;
+    it links nothing of the product;
+  * libsol_dropin.so (oracle/_ref/): the GPU drop-in sol::GpuPathTracer over the
+    scenes of libsol_ref.so (drop-in tests only; it loads the product library).
 
 Only tests, the smoke check and bench.py's CPU-baseline leg use this package.
 """
@@ -20,24 +23,27 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "_build" / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libsol_ref.so"
-# SoL's source tree (read only); SOL_REFERENCE_DIR points elsewhere (e.g. a copy of its test scenes).
-REF_SOURCES = Path(os.environ.get("SOL_REFERENCE_DIR", "/root/reference"))
+DROPIN_LIB = HERE / "_ref" / "libsol_dropin.so"
+# SoL's source tree (read only): $SOL_REF_DIR, by default the directory
+# `reference` beside this repository's root (as oracle/Makefile assumes).
+REF_SOURCES = Path(os.environ.get("SOL_REF_DIR") or HERE.parent.parent / "reference")
 
 _oracle = None
 _ref = None
 
 
 def build(ref: bool = True) -> None:
-    """Builds liboracle.so, and libsol_ref.so when SoL's sources are present."""
+    """Builds liboracle.so, and libsol_ref.so / libsol_dropin.so when SoL's
+    sources are present."""
     targets = ["oracle"]
     if ref and (REF_SOURCES / "src" / "algorithms" / "path_tracer.cpp").exists():
-        targets.append("ref")
-    subprocess.run(["make", "-s", "-C", str(HERE)] + targets, check=True)
+        targets += ["ref", "dropin"]
+    subprocess.run(["make", "-s", "-C", str(HERE), f"SOL_REF_DIR={REF_SOURCES}"] + targets, check=True)
 
 
 def _bind_common():
-    from sol_b200 import capi
-    return capi
+    from sol_b200 import abi
+    return abi
 
 
 class CameraArgs(C.Structure):
@@ -114,9 +120,6 @@ def ref_lib() -> C.CDLL:
         lib.ref_scene_render.restype = C.c_int
         lib.ref_scene_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p]
         lib.ref_scene_trace.restype = C.c_int
-        lib.ref_adapter_render.argtypes = [C.c_void_p, C.POINTER(capi.SolGpuConfig), C.c_uint64, C.c_uint32,
-                                           C.c_uint32, C.c_uint32, f32p, f32p, f32p, C.c_int, C.c_int, C.c_uint32]
-        lib.ref_adapter_render.restype = C.c_int
         lib.ref_renderjob_render.argtypes = [C.c_void_p, C.POINTER(capi.SolGpuConfig), C.c_uint32, C.c_uint32,
                                              C.c_uint32, C.c_uint32, f32p, f32p, f32p, C.c_int]
         lib.ref_renderjob_render.restype = C.c_int
@@ -128,6 +131,30 @@ def ref_lib() -> C.CDLL:
         lib.ref_scene_counts.restype = None
         _ref = lib
     return _ref
+
+
+_dropin = None
+
+
+def dropin_available() -> bool:
+    return DROPIN_LIB.exists()
+
+
+def dropin_lib() -> C.CDLL:
+    """libsol_dropin.so (loads libsol_ref.so and the product library)."""
+    global _dropin
+    if _dropin is None:
+        if not DROPIN_LIB.exists():
+            raise FileNotFoundError(f"{DROPIN_LIB} is not built (needs SoL's sources; see oracle/Makefile)")
+        capi = _bind_common()
+        ref_lib()
+        lib = C.CDLL(str(DROPIN_LIB))
+        f32p = C.POINTER(C.c_float)
+        lib.ref_adapter_render.argtypes = [C.c_void_p, C.POINTER(capi.SolGpuConfig), C.c_uint64, C.c_uint32,
+                                           C.c_uint32, C.c_uint32, f32p, f32p, f32p, C.c_int, C.c_int, C.c_uint32]
+        lib.ref_adapter_render.restype = C.c_int
+        _dropin = lib
+    return _dropin
 
 
 def _film(w: int, h: int, film=None) -> np.ndarray:
@@ -233,7 +260,7 @@ class RefScene:
         """The same sol::Scene rendered by sol::GpuPathTracer (the product's drop-in)."""
         out = _film(width, height, film)
         cfg = config.to_c()
-        rc = self.lib.ref_adapter_render(self.h, C.byref(cfg), sample_index, spp, width, height, *_ptrs(out),
+        rc = dropin_lib().ref_adapter_render(self.h, C.byref(cfg), sample_index, spp, width, height, *_ptrs(out),
                                          device, int(render_job), samples_per_frame or spp)
         if rc != 0:
             raise RuntimeError("sol::GpuPathTracer failed: " + self.lib.ref_last_error().decode())

@@ -26,8 +26,8 @@
 #include "sol/textures.h"
 #include "sol/triangle_mesh.h"
 
-#include "adapter/gpu_path_tracer.h"
 #include "oracle_camera.h"
+#include "ref_harness.h"
 #include "sol_gpu.h"
 
 // SoL's EXR support needs tinyexr, which is not vendored; the path tracer never
@@ -54,13 +54,12 @@ std::unique_ptr<sol::Texture> image_texture(const sol::Image& img, int border) {
 
 }  // namespace
 
-struct RefScene {
-    sol::Scene scene;
-};
 
 extern "C" {
 
 const char* ref_last_error(void) { return g_err.c_str(); }
+
+void ref_set_error(const char* what) { g_err = what; }
 
 RefScene* ref_scene_create(const SolGpuSceneDesc* d, const OracleCamera* cam) {
     try {
@@ -194,42 +193,6 @@ int ref_scene_render(RefScene* rs, const SolGpuConfig* cfg, uint64_t sample_inde
     if (render_ms) *render_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
     for (int ch = 0; ch < 3; ++ch) std::memcpy(film[ch], image.channel(ch).get(), sizeof(float) * n);
     return 0;
-}
-
-/// The same scene rendered by the GPU drop-in, sol::GpuPathTracer, optionally
-/// driven by sol::RenderJob (src/render_job.cpp:23-40) with `samples_per_frame`.
-/// Films are added into like ref_scene_render.  Returns 0, or -1 with the
-/// exception text in ref_last_error().
-int ref_adapter_render(RefScene* rs, const SolGpuConfig* cfg, uint64_t sample_index, uint32_t sample_count,
-                       uint32_t width, uint32_t height, float* r, float* g, float* b, int device,
-                       int use_render_job, uint32_t samples_per_frame) {
-    try {
-        sol::PathTracer::Config c;
-        c.max_path_len = cfg->max_path_len;
-        c.min_rr_path_len = cfg->min_rr_path_len;
-        c.min_survival_prob = cfg->min_survival_prob;
-        c.max_survival_prob = cfg->max_survival_prob;
-        c.ray_offset = cfg->ray_offset;
-        sol::GpuPathTracer tracer(rs->scene, c, device);
-        sol::Image image(width, height, 3);
-        float* film[3] = {r, g, b};
-        const size_t n = (size_t)width * height;
-        for (int ch = 0; ch < 3; ++ch) std::memcpy(image.channel(ch).get(), film[ch], sizeof(float) * n);
-        if (use_render_job) {
-            sol::RenderJob job(tracer, image);
-            job.sample_count = sample_count;
-            job.samples_per_frame = samples_per_frame;
-            job.start();
-            job.wait();
-        } else {
-            tracer.render(image, sample_index, sample_count);
-        }
-        for (int ch = 0; ch < 3; ++ch) std::memcpy(film[ch], image.channel(ch).get(), sizeof(float) * n);
-        return 0;
-    } catch (const std::exception& e) {
-        g_err = e.what();
-        return -1;
-    }
 }
 
 /// sol::PathTracer driven by sol::RenderJob, for comparison with the above.

@@ -4,9 +4,13 @@
 // SoL keeps the parameters this needs in private members without accessors
 // (bsdfs.h:110,128-129,142,158-160, lights.h:107-108,133-134,
 // triangle_mesh.h:53-59, cameras.h:50-54).  Integrated into SoL, the class is
-// declared a friend of those classes.  Built against SoL's unmodified headers,
-// this file gets the same access by widening `private`/`protected` while it
-// includes them: the class layouts are unchanged, only access checking is.
+// declared a friend of those classes (`friend class GpuPathTracer;` in each,
+// the header patch INTEGRATION.md gives) and this file is compiled with
+// SOL_GPU_FRIEND_PATCH defined.  Without the patch -- the test build, against
+// SoL's unmodified headers -- it gets the same access by widening
+// `private`/`protected` while it includes them: the class layouts are
+// unchanged, only access checking is (a stand-in for the friend declarations,
+// not the integration).
 // TriangleMesh's hierarchy holder is defined only inside triangle_mesh.cpp
 // (src/triangle_mesh.cpp:27-28); its one-member definition is repeated here.
 
@@ -38,8 +42,10 @@
 #include <proto/vec.h>
 #include <bvh/bvh.h>
 
+#ifndef SOL_GPU_FRIEND_PATCH
 #define private public
 #define protected public
+#endif
 #include "sol/bsdfs.h"
 #include "sol/cameras.h"
 #include "sol/image.h"
@@ -48,8 +54,10 @@
 #include "sol/shapes.h"
 #include "sol/textures.h"
 #include "sol/triangle_mesh.h"
+#ifndef SOL_GPU_FRIEND_PATCH
 #undef private
 #undef protected
+#endif
 
 #include "gpu_path_tracer.h"
 

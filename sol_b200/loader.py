@@ -43,7 +43,7 @@ import tomllib
 
 import numpy as np
 
-from . import capi
+from . import abi
 from .scene import Bsdf, Camera, Light, Scene, Texture
 
 _libc = C.CDLL(None)
@@ -141,7 +141,7 @@ class _Builder:
         self._tex, self._bsdf, self._light = {}, {}, {}
 
     def texture(self, kind: int, value) -> int:
-        if kind == capi.TEX_CONSTANT:
+        if kind == abi.TEX_CONSTANT:
             key = (kind, float(_f32(value)))
             val = (key[1], 0.0, 0.0)
         else:
@@ -163,32 +163,32 @@ class _Builder:
         key = (tuple(map(float, v0)), tuple(map(float, v1)), tuple(map(float, v2)), tex)
         if key not in self._light:
             self._light[key] = len(self.lights)
-            self.lights.append(Light(capi.LIGHT_TRIANGLE, key[0], key[1], key[2], intensity_tex=tex))
+            self.lights.append(Light(abi.LIGHT_TRIANGLE, key[0], key[1], key[2], intensity_tex=tex))
         return self._light[key]
 
     def material_bsdf(self, m: _Material) -> int:
         """convert_material (obj.cpp:370-418); -1 for no BSDF."""
         if m.illum == 5:
-            return self.bsdf(capi.BSDF_MIRROR, (self.texture(capi.TEX_CONSTANT_COLOR, m.ks), -1, -1))
+            return self.bsdf(abi.BSDF_MIRROR, (self.texture(abi.TEX_CONSTANT_COLOR, m.ks), -1, -1))
         if m.illum == 7:
-            ks = self.texture(capi.TEX_CONSTANT_COLOR, m.ks)
-            kt = self.texture(capi.TEX_CONSTANT_COLOR, m.tf)
-            eta = self.texture(capi.TEX_CONSTANT, _f32(1.0) / _f32(m.ni) if m.ni != 0.0 else np.float32(np.inf))
-            return self.bsdf(capi.BSDF_GLASS, (ks, kt, eta))
+            ks = self.texture(abi.TEX_CONSTANT_COLOR, m.ks)
+            kt = self.texture(abi.TEX_CONSTANT_COLOR, m.tf)
+            eta = self.texture(abi.TEX_CONSTANT, _f32(1.0) / _f32(m.ni) if m.ni != 0.0 else np.float32(np.inf))
+            return self.bsdf(abi.BSDF_GLASS, (ks, kt, eta))
         diff = spec = -1
         diff_k = spec_k = _f32(0.0)
         if not _is_black(m.ks) or m.map_ks:
-            ks = self.texture(capi.TEX_CONSTANT_COLOR, m.ks)
-            ns = self.texture(capi.TEX_CONSTANT, m.ns)
-            spec = self.bsdf(capi.BSDF_PHONG, (ks, ns, -1))
+            ks = self.texture(abi.TEX_CONSTANT_COLOR, m.ks)
+            ns = self.texture(abi.TEX_CONSTANT, m.ns)
+            spec = self.bsdf(abi.BSDF_PHONG, (ks, ns, -1))
             spec_k = _f32(1.0) if m.map_ks else _luminance(m.ks)
         if not _is_black(m.kd) or m.map_kd:
-            kd = self.texture(capi.TEX_CONSTANT_COLOR, m.kd)
-            diff = self.bsdf(capi.BSDF_DIFFUSE, (kd, -1, -1))
+            kd = self.texture(abi.TEX_CONSTANT_COLOR, m.kd)
+            diff = self.bsdf(abi.BSDF_DIFFUSE, (kd, -1, -1))
             diff_k = _f32(1.0) if m.map_kd else _luminance(m.kd)
         if spec >= 0 and diff >= 0:
-            k = self.texture(capi.TEX_CONSTANT, _f32(spec_k / _f32(diff_k + spec_k)))
-            return self.bsdf(capi.BSDF_INTERP, (k, -1, -1), diff, spec)
+            k = self.texture(abi.TEX_CONSTANT, _f32(spec_k / _f32(diff_k + spec_k)))
+            return self.bsdf(abi.BSDF_INTERP, (k, -1, -1), diff, spec)
         return diff if diff >= 0 else spec
 
 
@@ -281,7 +281,7 @@ def _load_obj(path: str, b: _Builder):
             nxt = vindex[idx[i + 1]]
             light = -1
             if emissive:
-                tex = b.texture(capi.TEX_CONSTANT_COLOR, m.ke)
+                tex = b.texture(abi.TEX_CONSTANT_COLOR, m.ke)
                 light = b.light(V[first], V[cur], V[nxt], tex)
             tris.append((first, cur, nxt))
             tri_bsdf.append(bsdf)

@@ -12,7 +12,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import capi
+from . import abi
 
 
 @dataclass
@@ -20,8 +20,8 @@ class Texture:
     type: int
     value: tuple = (0.0, 0.0, 0.0)
     image: int = -1
-    filter: int = capi.FILTER_BILINEAR
-    border: int = capi.BORDER_REPEAT
+    filter: int = abi.FILTER_BILINEAR
+    border: int = abi.BORDER_REPEAT
 
 
 @dataclass
@@ -51,9 +51,10 @@ class Camera:
     fov: float
     aspect: float
 
-    def to_c(self) -> capi.SolGpuCamera:
+    def to_c(self) -> abi.SolGpuCamera:
         """The constructed camera (sol_gpu_camera_perspective)."""
-        c = capi.SolGpuCamera()
+        from . import capi   # loads the CUDA library's C ABI
+        c = abi.SolGpuCamera()
         v3 = C.c_float * 3
         capi.check(capi.lib.sol_gpu_camera_perspective(v3(*self.eye), v3(*self.dir), v3(*self.up), self.fov,
                                                        self.aspect, C.byref(c)), "sol_gpu_camera_perspective")
@@ -69,8 +70,8 @@ class Config:
     max_survival_prob: float = 0.75
     ray_offset: float = 1e-5
 
-    def to_c(self) -> capi.SolGpuConfig:
-        c = capi.SolGpuConfig()
+    def to_c(self) -> abi.SolGpuConfig:
+        c = abi.SolGpuConfig()
         c.max_path_len = self.max_path_len
         c.min_rr_path_len = self.min_rr_path_len
         c.min_survival_prob = self.min_survival_prob
@@ -117,7 +118,7 @@ class SceneDesc:
         self.b = np.ascontiguousarray(s.tri_bsdf, dtype=np.int32)
         self.l = np.ascontiguousarray(s.tri_light, dtype=np.int32)
         self.imgs = [np.ascontiguousarray(im, dtype=np.float32) for im in s.images]
-        d = capi.SolGpuSceneDesc()
+        d = abi.SolGpuSceneDesc()
         d.num_vertices = self.v.shape[0]
         d.num_triangles = self.i.shape[0]
         d.vertices = _ptr(self.v, C.c_float)
@@ -126,20 +127,20 @@ class SceneDesc:
         d.indices = _ptr(self.i, C.c_uint32)
         d.tri_bsdf = _ptr(self.b, C.c_int32)
         d.tri_light = _ptr(self.l, C.c_int32)
-        self.tex_arr = (capi.SolGpuTexture * max(1, len(s.textures)))()
+        self.tex_arr = (abi.SolGpuTexture * max(1, len(s.textures)))()
         for k, t in enumerate(s.textures):
             self.tex_arr[k].type = t.type
             self.tex_arr[k].filter = t.filter
             self.tex_arr[k].border = t.border
             self.tex_arr[k].image = t.image
             self.tex_arr[k].value[:] = tuple(float(x) for x in t.value)
-        self.bsdf_arr = (capi.SolGpuBsdf * max(1, len(s.bsdfs)))()
+        self.bsdf_arr = (abi.SolGpuBsdf * max(1, len(s.bsdfs)))()
         for k, b in enumerate(s.bsdfs):
             self.bsdf_arr[k].type = b.type
             self.bsdf_arr[k].tex[:] = b.tex
             self.bsdf_arr[k].a = b.a
             self.bsdf_arr[k].b = b.b
-        self.light_arr = (capi.SolGpuLight * max(1, len(s.lights)))()
+        self.light_arr = (abi.SolGpuLight * max(1, len(s.lights)))()
         for k, li in enumerate(s.lights):
             L = self.light_arr[k]
             L.type = li.type
@@ -148,7 +149,7 @@ class SceneDesc:
             L.v0[:] = tuple(float(x) for x in li.v0)
             L.v1[:] = tuple(float(x) for x in li.v1)
             L.v2[:] = tuple(float(x) for x in li.v2)
-        self.img_arr = (capi.SolGpuImage * max(1, len(self.imgs)))()
+        self.img_arr = (abi.SolGpuImage * max(1, len(self.imgs)))()
         for k, im in enumerate(self.imgs):
             self.img_arr[k].height = im.shape[1]
             self.img_arr[k].width = im.shape[2]
@@ -181,8 +182,9 @@ def build_bvh(s: Scene):
     i = np.ascontiguousarray(s.indices, dtype=np.uint32)
     nt = i.shape[0]
     count = C.c_uint32(max(1, 2 * nt))
-    nodes = (capi.SolGpuBvhNode * max(1, 2 * nt))()
+    nodes = (abi.SolGpuBvhNode * max(1, 2 * nt))()
     prims = np.zeros(max(1, nt), dtype=np.uint32)
+    from . import capi   # loads the CUDA library's C ABI
     capi.check(capi.lib.sol_gpu_build_bvh(_ptr(v, C.c_float), v.shape[0], _ptr(i, C.c_uint32), nt, nodes,
                                           C.byref(count), _ptr(prims, C.c_uint32)), "sol_gpu_build_bvh")
     return nodes, count.value, prims[:nt]

@@ -20,7 +20,7 @@ import math
 
 import numpy as np
 
-from . import capi
+from . import abi
 from .scene import Bsdf, Camera, Config, Light, Scene, Texture
 
 M32 = 0xFFFFFFFF
@@ -181,23 +181,23 @@ def cornell_box(seed: int = 0, textured: bool = False, tex_size: int = 256, tex_
     """
     rng = Pcg(seed)
     tex = [
-        Texture(capi.TEX_CONSTANT_COLOR, (0.73, 0.73, 0.73)),   # 0 white
-        Texture(capi.TEX_CONSTANT_COLOR, (0.65, 0.05, 0.05)),   # 1 red
-        Texture(capi.TEX_CONSTANT_COLOR, (0.12, 0.45, 0.15)),   # 2 green
-        Texture(capi.TEX_CONSTANT_COLOR, (0.78, 0.78, 0.78)),   # 3 light surface
-        Texture(capi.TEX_CONSTANT_COLOR, (17.0, 12.0, 4.0)),    # 4 emission
-        Texture(capi.TEX_CONSTANT_COLOR, (1.0, 1.0, 1.0)),      # 5 glass ks / kt
-        Texture(capi.TEX_CONSTANT, (1.0 / 1.5, 0.0, 0.0)),      # 6 glass eta (1 / IOR)
-        Texture(capi.TEX_CONSTANT_COLOR, (0.5, 0.5, 0.5)),      # 7 phong ks
-        Texture(capi.TEX_CONSTANT, (64.0, 0.0, 0.0)),           # 8 phong ns
+        Texture(abi.TEX_CONSTANT_COLOR, (0.73, 0.73, 0.73)),   # 0 white
+        Texture(abi.TEX_CONSTANT_COLOR, (0.65, 0.05, 0.05)),   # 1 red
+        Texture(abi.TEX_CONSTANT_COLOR, (0.12, 0.45, 0.15)),   # 2 green
+        Texture(abi.TEX_CONSTANT_COLOR, (0.78, 0.78, 0.78)),   # 3 light surface
+        Texture(abi.TEX_CONSTANT_COLOR, (17.0, 12.0, 4.0)),    # 4 emission
+        Texture(abi.TEX_CONSTANT_COLOR, (1.0, 1.0, 1.0)),      # 5 glass ks / kt
+        Texture(abi.TEX_CONSTANT, (1.0 / 1.5, 0.0, 0.0)),      # 6 glass eta (1 / IOR)
+        Texture(abi.TEX_CONSTANT_COLOR, (0.5, 0.5, 0.5)),      # 7 phong ks
+        Texture(abi.TEX_CONSTANT, (64.0, 0.0, 0.0)),           # 8 phong ns
     ]
     bsdfs = [
-        Bsdf(capi.BSDF_DIFFUSE, (0, -1, -1)),    # 0 white
-        Bsdf(capi.BSDF_DIFFUSE, (1, -1, -1)),    # 1 red
-        Bsdf(capi.BSDF_DIFFUSE, (2, -1, -1)),    # 2 green
-        Bsdf(capi.BSDF_DIFFUSE, (3, -1, -1)),    # 3 light surface
-        Bsdf(capi.BSDF_GLASS, (5, 5, 6)),        # 4 glass
-        Bsdf(capi.BSDF_PHONG, (7, 8, -1)),       # 5 phong
+        Bsdf(abi.BSDF_DIFFUSE, (0, -1, -1)),    # 0 white
+        Bsdf(abi.BSDF_DIFFUSE, (1, -1, -1)),    # 1 red
+        Bsdf(abi.BSDF_DIFFUSE, (2, -1, -1)),    # 2 green
+        Bsdf(abi.BSDF_DIFFUSE, (3, -1, -1)),    # 3 light surface
+        Bsdf(abi.BSDF_GLASS, (5, 5, 6)),        # 4 glass
+        Bsdf(abi.BSDF_PHONG, (7, 8, -1)),       # 5 phong
     ]
     images = []
     back_bsdf = floor_bsdf = 0
@@ -206,9 +206,9 @@ def cornell_box(seed: int = 0, textured: bool = False, tex_size: int = 256, tex_
             images = [np.asarray(t, np.float32) for t in textures_override]
         else:
             images = [noise_texture(tex_size, tex_seed), noise_texture(tex_size, tex_seed + 1)]
-        tex += [Texture(capi.TEX_IMAGE, image=0, filter=capi.FILTER_BILINEAR, border=capi.BORDER_REPEAT),   # 9 back
-                Texture(capi.TEX_IMAGE, image=1, filter=capi.FILTER_BILINEAR, border=capi.BORDER_REPEAT)]   # 10 floor
-        bsdfs += [Bsdf(capi.BSDF_DIFFUSE, (9, -1, -1)), Bsdf(capi.BSDF_DIFFUSE, (10, -1, -1))]
+        tex += [Texture(abi.TEX_IMAGE, image=0, filter=abi.FILTER_BILINEAR, border=abi.BORDER_REPEAT),   # 9 back
+                Texture(abi.TEX_IMAGE, image=1, filter=abi.FILTER_BILINEAR, border=abi.BORDER_REPEAT)]   # 10 floor
+        bsdfs += [Bsdf(abi.BSDF_DIFFUSE, (9, -1, -1)), Bsdf(abi.BSDF_DIFFUSE, (10, -1, -1))]
         back_bsdf, floor_bsdf = 6, 7
 
     mb = MeshBuilder()
@@ -223,8 +223,8 @@ def cornell_box(seed: int = 0, textured: bool = False, tex_size: int = 256, tex_
     y = 1.0 - 1e-4
     l0, l1, l2, l3 = (0.375, y, 0.375), (0.625, y, 0.375), (0.625, y, 0.625), (0.375, y, 0.625)
     mb.quad(l0, l1, l2, l3, 3, light_ids=[0, 1])
-    lights = [Light(capi.LIGHT_TRIANGLE, l0, l1, l2, intensity_tex=4),
-              Light(capi.LIGHT_TRIANGLE, l0, l2, l3, intensity_tex=4)]
+    lights = [Light(abi.LIGHT_TRIANGLE, l0, l1, l2, intensity_tex=4),
+              Light(abi.LIGHT_TRIANGLE, l0, l2, l3, intensity_tex=4)]
     # Boxes: glass 0.3^3 on the image's right half, Phong 0.3 x 0.6 x 0.3 on the left.
     gx, gz, ga = rng.uniform(0.22, 0.42), rng.uniform(0.25, 0.45), rng.uniform(0.0, math.pi / 2)
     px, pz, pa = rng.uniform(0.58, 0.78), rng.uniform(0.55, 0.75), rng.uniform(0.0, math.pi / 2)
@@ -295,14 +295,14 @@ def sphere_field(num_spheres: int = 64, seed: int = 1, bands: int = 65, segments
     tex, bsdfs, lights, images = [], [], [], []
     mb = MeshBuilder()
     # Ground: diffuse 0.5.
-    tex.append(Texture(capi.TEX_CONSTANT_COLOR, (0.5, 0.5, 0.5)))
-    bsdfs.append(Bsdf(capi.BSDF_DIFFUSE, (0, -1, -1)))
+    tex.append(Texture(abi.TEX_CONSTANT_COLOR, (0.5, 0.5, 0.5)))
+    bsdfs.append(Bsdf(abi.BSDF_DIFFUSE, (0, -1, -1)))
     g0, g1 = -2.0 * box, 3.0 * box
     mb.quad((g0, 0, g0), (g0, 0, g1), (g1, 0, g1), (g1, 0, g0), 0, uv=((0, 0), (0, 1), (1, 1), (1, 0)))
     if textured:
         images.append(noise_texture(tex_size, seed + 17))
-        tex.append(Texture(capi.TEX_IMAGE, image=0, filter=capi.FILTER_BILINEAR, border=capi.BORDER_REPEAT))
-        bsdfs.append(Bsdf(capi.BSDF_DIFFUSE, (len(tex) - 1, -1, -1)))
+        tex.append(Texture(abi.TEX_IMAGE, image=0, filter=abi.FILTER_BILINEAR, border=abi.BORDER_REPEAT))
+        bsdfs.append(Bsdf(abi.BSDF_DIFFUSE, (len(tex) - 1, -1, -1)))
     cache = {}
     for k in range(num_spheres):
         px, py, pz = rng.uniform(0, box), rng(), rng.uniform(0, box)
@@ -314,21 +314,21 @@ def sphere_field(num_spheres: int = 64, seed: int = 1, bands: int = 65, segments
             if textured and k % 2 == 0:
                 b = 1   # the image-textured diffuse BSDF
             else:
-                tex.append(Texture(capi.TEX_CONSTANT_COLOR, albedo))
-                bsdfs.append(Bsdf(capi.BSDF_DIFFUSE, (len(tex) - 1, -1, -1)))
+                tex.append(Texture(abi.TEX_CONSTANT_COLOR, albedo))
+                bsdfs.append(Bsdf(abi.BSDF_DIFFUSE, (len(tex) - 1, -1, -1)))
                 b = len(bsdfs) - 1
         elif kind == 1:
             ns = math.exp(rng.uniform(0.0, math.log(1000.0)))
             ks = rng.uniform(0.0, 0.5)
-            tex.append(Texture(capi.TEX_CONSTANT_COLOR, (ks, ks, ks)))
-            tex.append(Texture(capi.TEX_CONSTANT, (ns, 0.0, 0.0)))
-            bsdfs.append(Bsdf(capi.BSDF_PHONG, (len(tex) - 2, len(tex) - 1, -1)))
+            tex.append(Texture(abi.TEX_CONSTANT_COLOR, (ks, ks, ks)))
+            tex.append(Texture(abi.TEX_CONSTANT, (ns, 0.0, 0.0)))
+            bsdfs.append(Bsdf(abi.BSDF_PHONG, (len(tex) - 2, len(tex) - 1, -1)))
             b = len(bsdfs) - 1
         else:
             ior = rng.uniform(1.3, 1.8)
-            tex.append(Texture(capi.TEX_CONSTANT_COLOR, (1.0, 1.0, 1.0)))
-            tex.append(Texture(capi.TEX_CONSTANT, (1.0 / ior, 0.0, 0.0)))
-            bsdfs.append(Bsdf(capi.BSDF_GLASS, (len(tex) - 2, len(tex) - 2, len(tex) - 1)))
+            tex.append(Texture(abi.TEX_CONSTANT_COLOR, (1.0, 1.0, 1.0)))
+            tex.append(Texture(abi.TEX_CONSTANT, (1.0 / ior, 0.0, 0.0)))
+            bsdfs.append(Bsdf(abi.BSDF_GLASS, (len(tex) - 2, len(tex) - 2, len(tex) - 1)))
             b = len(bsdfs) - 1
         nb, ns_ = sphere_sizes[k] if sphere_sizes is not None else (bands, segments)
         if (nb, ns_) not in cache:
@@ -337,20 +337,20 @@ def sphere_field(num_spheres: int = 64, seed: int = 1, bands: int = 65, segments
         disp = 1.0 + 0.1 * fractal_noise(uv_v * 2.0 + 13.0 * k, seed * 1000 + k)
         v = uv_v * (disp * scale)[:, None] + np.array([px, py, pz])
         mb.add(v, _smooth_normals(v, uv_t), uv_uv, uv_t, b)
-    tex.append(Texture(capi.TEX_CONSTANT_COLOR, (0.8, 0.8, 0.8)))
+    tex.append(Texture(abi.TEX_CONSTANT_COLOR, (0.8, 0.8, 0.8)))
     light_surface = len(bsdfs)
-    bsdfs.append(Bsdf(capi.BSDF_DIFFUSE, (len(tex) - 1, -1, -1)))
+    bsdfs.append(Bsdf(abi.BSDF_DIFFUSE, (len(tex) - 1, -1, -1)))
     y = box + 1.0
     for cx, cz in ((0.25, 0.25), (0.75, 0.25), (0.25, 0.75), (0.75, 0.75)):
         e = rng.uniform(5.0, 20.0)
-        tex.append(Texture(capi.TEX_CONSTANT_COLOR, (e, e, e)))
+        tex.append(Texture(abi.TEX_CONSTANT_COLOR, (e, e, e)))
         x0, x1 = cx * box - 1.0, cx * box + 1.0
         z0, z1 = cz * box - 1.0, cz * box + 1.0
         q = ((x0, y, z0), (x1, y, z0), (x1, y, z1), (x0, y, z1))   # faces -y
         base = len(lights)
         mb.quad(*q, light_surface, light_ids=[base, base + 1])
-        lights.append(Light(capi.LIGHT_TRIANGLE, q[0], q[1], q[2], intensity_tex=len(tex) - 1))
-        lights.append(Light(capi.LIGHT_TRIANGLE, q[0], q[2], q[3], intensity_tex=len(tex) - 1))
+        lights.append(Light(abi.LIGHT_TRIANGLE, q[0], q[1], q[2], intensity_tex=len(tex) - 1))
+        lights.append(Light(abi.LIGHT_TRIANGLE, q[0], q[2], q[3], intensity_tex=len(tex) - 1))
     cam = Camera(eye=(0.5 * box, 0.7 * box, -0.7 * box), dir=(0.0, -0.4 * box, 1.2 * box), up=(0.0, 1.0, 0.0),
                  fov=60.0, aspect=aspect)
     return mb.scene(textures=tex, bsdfs=bsdfs, lights=lights, images=images, camera=cam)

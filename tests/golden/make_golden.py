@@ -7,7 +7,8 @@
                     and the classes it uses, built by oracle/Makefile against the
                     clean-room proto/par/bvh shims) on small seeded scenes.
 
-Needs SoL's sources at /root/reference (or SOL_REF_DIR); run from the repo root:
+Needs SoL's sources in $SOL_REF_DIR (by default the directory `reference`
+beside the repository's root); run from the repo root:
     python tests/golden/make_golden.py
 """
 from __future__ import annotations
@@ -24,7 +25,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
-SOL = Path(os.environ.get("SOL_REF_DIR", "/root/reference"))
+SOL = Path(os.environ.get("SOL_REF_DIR") or ROOT.parent / "reference")
 
 PCG_SEEDS = [0, 1, 42, 0xDEADBEEF, 2**32 - 1, 123456789]
 PCG_DRAWS = 64

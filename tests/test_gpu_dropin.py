@@ -10,7 +10,7 @@ import oracle
 from helpers import per_pixel_parity
 
 pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(not oracle.ref_available(), reason="SoL's sources were not built into oracle/_ref")]
+              pytest.mark.skipif(not oracle.dropin_available(), reason="SoL's sources were not built into oracle/_ref")]
 
 
 def test_dropin_matches_sol_pathtracer_cornell(built):

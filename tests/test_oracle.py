@@ -86,3 +86,21 @@ def test_oracle_matches_sol_pathtracer_accumulation(built):
     b, _ = ref.render(cfg, 16, 16, 3, 2, film=b)
     exact, bad = per_pixel_parity(a, b)
     assert bad == 0 and exact >= 0.99
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="SoL's sources were not built into oracle/_ref")
+def test_reference_library_links_nothing_of_the_product():
+    """The timed CPU reference (SoL's PathTracer in libsol_ref.so) must not map
+    the product library: its dynamic section needs no libsol_gpu.so, and
+    building a scene for it loads no CUDA library into the process."""
+    import subprocess
+    import sys
+    out = subprocess.run(["readelf", "-d", str(oracle.REF_LIB)], capture_output=True, text=True, check=True).stdout
+    needed = [l for l in out.splitlines() if "(NEEDED)" in l]
+    assert needed and not any("sol_gpu" in l or "cuda" in l.lower() for l in needed), needed
+    code = ("import sys; sys.path.insert(0, '.'); import oracle; from sol_b200 import scenes; "
+            "s = scenes.cornell_box(0); r = oracle.RefScene(s); r.render(scenes.CORNELL_CONFIG, 8, 8, 1); "
+            "maps = open('/proc/self/maps').read(); "
+            "assert 'libsol_gpu' not in maps and 'libcuda' not in maps, 'product library mapped'; "
+            "assert 'sol_b200.capi' not in sys.modules")
+    subprocess.run([sys.executable, "-c", code], check=True, cwd=str(Path(__file__).resolve().parent.parent))
