@@ -282,6 +282,15 @@ int sol_gpu_scene_set_schedule(SolGpuScene* scene, int schedule);
  * counterpart in the reference (SoL renders on the host). */
 int sol_gpu_scene_set_scratch_limit(SolGpuScene* scene, uint64_t bytes);
 
+/* Self-check bound of the BVH traversal on this scene, for tests of the error
+ * path (0 restores the default, 2 x (nodes + triangles) + 16 loop steps, which
+ * no valid hierarchy reaches).  A ray whose traversal exceeds it is dropped,
+ * the kernel records the fault instead of looping, and the render (or the
+ * stats call after it) fails with SOL_GPU_ERR_BAD_INDEX; the next render
+ * starts clean.  Applies to renders, traces and batches issued afterwards.
+ * Replaces no SoL interface: SoL's traversal has no bound (it cannot fail). */
+int sol_gpu_scene_set_traversal_limit(SolGpuScene* scene, uint32_t max_steps);
+
 /* Closest-hit (any_hit == 0) or any-hit (any_hit != 0) queries for a batch of
  * device-resident rays, the device side of TriangleMesh::intersect_closest /
  * intersect_any (src/triangle_mesh.cpp:64-117).  Asynchronous on `stream`. */
@@ -340,8 +349,24 @@ int sol_gpu_batch_destroy(SolGpuBatch* batch);
 int sol_gpu_batch_render(SolGpuBatch* batch, const SolGpuConfig* config, const SolGpuView* views,
                          uint32_t num_views, void* stream);
 
-/* Counters and device time of the last batch render (waits for it). */
+/* Counters and device time of the last batch render (waits for it).  Fails
+ * with SOL_GPU_ERR_TIMEOUT when the wavefront's bounce loop hit its iteration
+ * bound, and with SOL_GPU_ERR_BAD_INDEX when a kernel self-check fired. */
 int sol_gpu_batch_stats(SolGpuBatch* batch, SolGpuRenderStats* out);
+
+/* Limit on the wavefront's scratch for one render of this batch, in bytes (0:
+ * the default, 8 GiB): per-sample colours of every (view, sample, pixel) and,
+ * when they do not fit, the pixel sums carried between chunks of samples that
+ * fit.  The film bits do not change.  No counterpart in the reference. */
+int sol_gpu_batch_set_scratch_limit(SolGpuBatch* batch, uint64_t bytes);
+
+/* Self-check bound on the wavefront's bounce-loop iterations per render, for
+ * tests of the error path (0 restores the default: every vertex of every
+ * sample, plus one iteration per sample, which no render reaches).  A render
+ * that reaches it stops, and sol_gpu_batch_stats reports SOL_GPU_ERR_TIMEOUT;
+ * the next render starts clean.  No counterpart in SoL (RenderJob::wait's
+ * timeout, src/render_job.cpp:42-55, bounds a host wait, not the loop). */
+int sol_gpu_batch_set_iteration_limit(SolGpuBatch* batch, uint64_t max_iterations);
 
 /* Times candidate options (capacity, block size, binning threshold; with
  * schedule AUTO also the megakernel schedule) on one sample per pixel of the
@@ -464,6 +489,12 @@ int sol_gpu_batch_forward_adjoint(SolGpuBatch* batch, const SolGpuConfig* config
  * array, so calls that can overlap on the GPU (different streams without
  * ordering, different host threads) race: order them.  The first call on a
  * device looks up the array's address; make it before any stream capture.
+ * The tables reach the array as kernel parameters of a small copy kernel (no
+ * copy from pageable host memory).  With lazy module loading (the CUDA 12
+ * default) the library's device image and the array become resident on a
+ * device at the library's first launch there, or when the library is loaded
+ * under CUDA_MODULE_LOADING=EAGER; the address is cached per device, so the
+ * library must not be used after cudaDeviceReset in the same process.
  * Requires config->max_path_len <= 16.  Asynchronous. */
 int sol_gpu_batch_forward_adjoint_noalloc(SolGpuScene* const* scenes, uint32_t num_scenes,
                                           const SolGpuConfig* config, const SolGpuAdjointView* views,

@@ -134,6 +134,7 @@ SIGNATURES = [
     ("sol_gpu_scene_set_instrumented", C.c_int, [ScenePtr, C.c_int]),
     ("sol_gpu_scene_set_schedule", C.c_int, [ScenePtr, C.c_int]),
     ("sol_gpu_scene_set_scratch_limit", C.c_int, [ScenePtr, C.c_uint64]),
+    ("sol_gpu_scene_set_traversal_limit", C.c_int, [ScenePtr, C.c_uint32]),
     ("sol_gpu_trace", C.c_int, [ScenePtr, C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]),
     ("sol_gpu_batch_create", C.c_int, [C.POINTER(ScenePtr), C.c_uint32, C.POINTER(SolGpuBatchOptions),
                                        C.POINTER(BatchPtr)]),
@@ -141,6 +142,8 @@ SIGNATURES = [
     ("sol_gpu_batch_render", C.c_int, [BatchPtr, C.POINTER(SolGpuConfig), C.POINTER(SolGpuView), C.c_uint32,
                                        C.c_void_p]),
     ("sol_gpu_batch_stats", C.c_int, [BatchPtr, C.POINTER(SolGpuRenderStats)]),
+    ("sol_gpu_batch_set_iteration_limit", C.c_int, [BatchPtr, C.c_uint64]),
+    ("sol_gpu_batch_set_scratch_limit", C.c_int, [BatchPtr, C.c_uint64]),
     ("sol_gpu_batch_forward_adjoint", C.c_int, [BatchPtr, C.POINTER(SolGpuConfig), C.POINTER(SolGpuAdjointView),
                                                 C.c_uint32, C.c_void_p]),
     ("sol_gpu_batch_forward_adjoint_noalloc", C.c_int, [C.POINTER(ScenePtr), C.c_uint32, C.POINTER(SolGpuConfig),

@@ -21,6 +21,7 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 BUILD_DIR = PKG / "_build"
 LIB = LIB_DIR / "libsol_gpu.so"
+PROBE_LIB = LIB_DIR / "libsol_probe.so"   # memory probes for the roofline (bench only)
 
 CUDA_SOURCES = ["kernels/megakernel.cu", "kernels/trace.cu", "kernels/wavefront.cu", "kernels/adjoint.cu",
                 "kernels/lbvh.cu", "noalloc.cu"]
@@ -47,7 +48,7 @@ def _inputs() -> list[Path]:
 
 
 def up_to_date() -> bool:
-    if not LIB.exists():
+    if not LIB.exists() or not PROBE_LIB.exists():
         return False
     t = LIB.stat().st_mtime
     return all(p.stat().st_mtime <= t for p in _inputs())
@@ -90,6 +91,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     link = [cc, "-shared", "-o", str(LIB)] + [str(o) for _, o, _ in jobs] + ARCH + \
            ["-Xcompiler", "-fopenmp", "-lgomp"]
     _run(link)
+    _run([cc, "-shared", "-o", str(PROBE_LIB), str(CSRC / "probe.cu")] + NVCC_DEVICE + ["-Xcompiler", "-fPIC"])
     return LIB
 
 

@@ -36,8 +36,12 @@ struct SolGpuBatch {
     AdjView* d_adj_views = nullptr;
     size_t adj_views_cap = 0;
     DeviceCounters* d_dc = nullptr;   // counters of the megakernel-type launches
-    float* scratch = nullptr;         // per-sample colours of split views (megakernel schedule)
+    float* scratch = nullptr;         // per-sample colours of split views (and the wavefront's running sums)
     uint64_t scratch_floats = 0;
+    WfSceneTable wf_table{};          // the scenes as the wavefront stages take them (kernel parameter)
+    bool basic = false;               // every scene has basic shading
+    unsigned long long max_iterations = 0;   // wavefront bounce-loop bound (0: the default)
+    uint64_t scratch_limit = 0;       // wavefront scratch bytes per render (0: kWfScratchMaxBytes)
     WfLaunch launch{};
     int launch_block = 0;
     cudaGraph_t graph = nullptr;
@@ -47,6 +51,7 @@ struct SolGpuBatch {
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     bool rendered = false;
     bool last_dc = false;             // the last launch counted into d_dc (megakernel schedules)
+    uint32_t last_passes = 0;         // wavefront launches (sample chunks) of the last render
 };
 
 namespace {
@@ -58,11 +63,11 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 size_t pool_bytes(uint32_t c) {
     size_t b = 0;
-    b += 8 * align256(sizeof(float4) * (size_t)c);                    // ray_o ray_d thru color sum sh_o sh_d pending
+    b += 9 * align256(sizeof(float4) * (size_t)c);                    // thru color ray_o[2] ray_d[2] sh_o sh_d sh_c
     b += align256(sizeof(unsigned long long) * (size_t)c);            // rng
     b += align256(sizeof(uint4) * (size_t)c);                         // pix
     b += align256(sizeof(float2) * (size_t)c);                        // hit
-    b += (4 + kWfBins + 1) * align256(sizeof(uint32_t) * (size_t)c);  // queues
+    b += (2 + kWfBins) * align256(sizeof(uint32_t) * (size_t)c);      // ended queues, bins
     return b;
 }
 
@@ -86,24 +91,20 @@ int alloc_pool(SolGpuBatch* b, uint32_t capacity) {
     auto take = [&](size_t bytes) { char* r = p; p += align256(bytes); return r; };
     const size_t c = capacity;
     WfParams& h = b->host;
-    h.ray_o = reinterpret_cast<float4*>(take(sizeof(float4) * c));
-    h.ray_d = reinterpret_cast<float4*>(take(sizeof(float4) * c));
     h.thru = reinterpret_cast<float4*>(take(sizeof(float4) * c));
     h.color = reinterpret_cast<float4*>(take(sizeof(float4) * c));
-    h.sum = reinterpret_cast<float4*>(take(sizeof(float4) * c));
-    h.sh_o = reinterpret_cast<float4*>(take(sizeof(float4) * c));
-    h.sh_d = reinterpret_cast<float4*>(take(sizeof(float4) * c));
-    h.pending = reinterpret_cast<float4*>(take(sizeof(float4) * c));
     h.rng = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * c));
     h.pix = reinterpret_cast<uint4*>(take(sizeof(uint4) * c));
+    for (int k = 0; k < 2; ++k) {
+        h.ray_o[k] = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+        h.ray_d[k] = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+        h.q_ended[k] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
+    }
     h.hit = reinterpret_cast<float2*>(take(sizeof(float2) * c));
-    h.q_extend[0] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
-    h.q_extend[1] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
-    h.q_regen[0] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
-    h.q_regen[1] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
+    h.sh_o = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    h.sh_d = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    h.sh_c = reinterpret_cast<float4*>(take(sizeof(float4) * c));
     h.q_bins = reinterpret_cast<uint32_t*>(p);
-    p += kWfBins * align256(sizeof(uint32_t) * c);
-    h.q_shadow = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
     return SOL_GPU_OK;
 }
 
@@ -139,7 +140,7 @@ int build_graph(SolGpuBatch* b) {
     cudaGraph_t body = np.conditional.phGraph_out[0];
     e = cudaStreamBeginCaptureToGraph(b->capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        cudaError_t le = launch_wf_iteration(b->d_params, b->launch, handle, 1, b->capture);
+        cudaError_t le = launch_wf_iteration(b->d_params, b->wf_table, b->basic, b->launch, handle, 1, b->capture);
         e = cudaStreamEndCapture(b->capture, &body);
         if (e == cudaSuccess) e = le;
     }
@@ -203,6 +204,9 @@ int upload_views(SolGpuBatch* b, const SolGpuView* views, uint32_t n, uint32_t* 
         w.split = scratch_at[i] != 0;
         w.scratch = w.split ? b->scratch + (scratch_at[i] - 1) : nullptr;
         w.sum_begin = sum_at;
+        w.running = nullptr;
+        w.first_chunk = 1;
+        w.last_chunk = 1;
         if (w.split) sum_at += 3 * (uint64_t)s.width * s.height;
         items += (uint64_t)w.tiles_x * ((s.height + 3) / 4) * 32 * (w.split ? s.sample_count : 1u);
         px += (uint64_t)s.width * s.height;
@@ -224,13 +228,38 @@ int upload_views(SolGpuBatch* b, const SolGpuView* views, uint32_t n, uint32_t* 
     return SOL_GPU_OK;
 }
 
-int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* views, uint32_t n, cudaStream_t stream) {
+/// Largest scratch (per-sample colours and running sums) the wavefront may
+/// hold for one render; batches needing more run in chunks of samples.
+#ifndef SOL_WF_SCRATCH_MAX_MB
+#define SOL_WF_SCRATCH_MAX_MB 8192
+#endif
+constexpr uint64_t kWfScratchMaxBytes = uint64_t(SOL_WF_SCRATCH_MAX_MB) << 20;
+
+/// Re-reads the scenes' device views (their traversal bound may have changed
+/// since the batch was made) and refreshes the tables built from them.
+int refresh_scenes(SolGpuBatch* b) {
+    bool changed = false;
+    for (size_t i = 0; i < b->scenes.size(); ++i)
+        if (std::memcmp(&b->h_scenes[i], &b->scenes[i]->view, sizeof(SceneView)) != 0) {
+            b->h_scenes[i] = b->scenes[i]->view;
+            changed = true;
+        }
+    if (!changed) return SOL_GPU_OK;
+    cudaError_t e = cudaMemcpy(b->d_scenes, b->h_scenes.data(), sizeof(SceneView) * b->h_scenes.size(),
+                               cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "scene table upload");
+    for (size_t i = 0; i < b->h_scenes.size() && i < kWfMaxScenes; ++i) b->wf_table.v[i] = b->h_scenes[i];
+    destroy_graph(b);
+    return SOL_GPU_OK;
+}
+
+int render_megakernel(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* views, uint32_t n,
+                      cudaStream_t stream) {
     uint32_t total_items = 0;
     uint64_t pixels = 0, sum_floats = 0;
-    const bool mk = b->opts.schedule == SOL_GPU_BATCH_MEGAKERNEL;
-    int rc = upload_views(b, views, n, &total_items, &pixels, stream, mk, &sum_floats);
+    int rc = upload_views(b, views, n, &total_items, &pixels, stream, true, &sum_floats);
     if (rc != SOL_GPU_OK) return rc;
-    if (mk) {
+    {
         if (!b->d_dc) {
             cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_dc), sizeof(DeviceCounters));
             if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc counters");
@@ -257,53 +286,187 @@ int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* v
         b->last_dc = true;
         return SOL_GPU_OK;
     }
+}
+
+/// One launch of the wavefront over a set of views (one chunk of samples).
+struct WfPass {
+    size_t first_view = 0;   // into the concatenated view tables
+    uint32_t num_views = 0;
+    uint32_t total_items = 0;
+    uint64_t sum_floats = 0;
+};
+
+/// The wavefront: views are split into (sample, pixel) work items whose path
+/// colours go to per-sample scratch planes, summed per pixel in sample order
+/// afterwards.  When the scratch of every sample would exceed
+/// kWfScratchMaxBytes, the samples run in chunks of K (the largest K that
+/// fits): chunk j renders samples [jK, (j+1)K) of every view that has them,
+/// carrying each pixel's sum from chunk to chunk.
+int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* views, uint32_t n,
+                     cudaStream_t stream) {
+    if (b->scenes.size() > kWfMaxScenes)
+        return fail(SOL_GPU_ERR_UNSUPPORTED, "the wavefront schedule takes at most 64 scenes per batch");
+    uint32_t max_spp = 0;
+    uint64_t all_floats = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const SolGpuView& s = views[i];
+        if (s.scene >= b->scenes.size()) return fail(SOL_GPU_ERR_INVALID_ARG, "view scene index out of range");
+        if (s.width == 0 || s.height == 0) return fail(SOL_GPU_ERR_INVALID_ARG, "view size must be positive");
+        if (!s.film) return fail(SOL_GPU_ERR_INVALID_ARG, "view film must not be NULL");
+        max_spp = std::max(max_spp, s.sample_count);
+        all_floats += 3ull * s.width * s.height * s.sample_count;
+    }
+    const uint64_t limit = (b->scratch_limit ? b->scratch_limit : kWfScratchMaxBytes) / sizeof(float);
+    auto need = [&](uint32_t k) {   // scratch floats of chunks of k samples: first chunk + running sums
+        uint64_t f = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            const uint64_t plane = 3ull * views[i].width * views[i].height;
+            f += plane * std::min(k, views[i].sample_count);
+            if (views[i].sample_count > k) f += plane;
+        }
+        return f;
+    };
+    uint32_t chunk = std::max(max_spp, 1u);
+    if (all_floats > limit) {
+        if (need(1) > limit) return fail(SOL_GPU_ERR_OUT_OF_MEMORY, "batch films too large for the wavefront's scratch");
+        uint32_t lo = 1, hi = max_spp;   // largest k with need(k) <= limit
+        while (hi - lo > 1) { const uint32_t mid = lo + (hi - lo) / 2; if (need(mid) <= limit) lo = mid; else hi = mid; }
+        chunk = lo;
+    }
+    const uint64_t scratch_floats = std::max<uint64_t>(need(chunk), 1);
+    if (b->scratch_floats < scratch_floats) {
+        cudaFree(b->scratch);
+        b->scratch = nullptr;
+        b->scratch_floats = 0;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->scratch), scratch_floats * sizeof(float));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc wavefront scratch");
+        b->scratch_floats = scratch_floats;
+    }
+    // Running sums sit after the largest chunk's per-sample planes; each
+    // chunked view keeps its place across chunks.
+    std::vector<uint64_t> running_at(n, 0);
+    {
+        uint64_t at = 0;
+        for (uint32_t i = 0; i < n; ++i) at += 3ull * views[i].width * views[i].height * std::min(chunk, views[i].sample_count);
+        for (uint32_t i = 0; i < n; ++i)
+            if (views[i].sample_count > chunk) { running_at[i] = at; at += 3ull * views[i].width * views[i].height; }
+    }
+    std::vector<WfView> table;
+    std::vector<WfPass> passes;
+    uint64_t paths = 0;
+    for (uint32_t c0 = 0; c0 < max_spp; c0 += chunk) {
+        WfPass pass;
+        pass.first_view = table.size();
+        uint64_t items = 0, scratch_at = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            const SolGpuView& s = views[i];
+            if (s.sample_count <= c0) continue;
+            const uint32_t k = std::min(chunk, s.sample_count - c0);
+            WfView w{};
+            std::memcpy(w.eye, s.camera.eye, sizeof(w.eye));
+            std::memcpy(w.dir, s.camera.dir, sizeof(w.dir));
+            std::memcpy(w.right, s.camera.right, sizeof(w.right));
+            std::memcpy(w.up, s.camera.up, sizeof(w.up));
+            w.scene = s.scene;
+            w.width = s.width;
+            w.height = s.height;
+            w.sample_count = k;
+            w.sample_index = s.sample_index + c0;
+            w.film = s.film;
+            w.tiles_x = (s.width + 7) / 8;
+            w.item_begin = (uint32_t)items;
+            w.split = 1;
+            w.scratch = b->scratch + scratch_at;
+            w.sum_begin = pass.sum_floats;
+            w.running = s.sample_count > chunk ? b->scratch + running_at[i] : nullptr;
+            w.first_chunk = c0 == 0;
+            w.last_chunk = c0 + k >= s.sample_count;
+            const uint64_t plane3 = 3ull * s.width * s.height;
+            scratch_at += plane3 * k;
+            pass.sum_floats += plane3;
+            items += (uint64_t)w.tiles_x * ((s.height + 3) / 4) * 32 * k;
+            paths += (uint64_t)s.width * s.height * k;
+            if (items > 0xffffffffull) return fail(SOL_GPU_ERR_INVALID_ARG, "batch too large (more than 2^32 work items)");
+            table.push_back(w);
+        }
+        pass.num_views = (uint32_t)(table.size() - pass.first_view);
+        pass.total_items = (uint32_t)items;
+        passes.push_back(pass);
+    }
+    if (b->views_cap < table.size()) {
+        cudaFree(b->d_views);
+        b->d_views = nullptr;
+        b->views_cap = 0;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->d_views), sizeof(WfView) * std::max<size_t>(table.size(), 64));
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc views");
+        b->views_cap = std::max<size_t>(table.size(), 64);
+    }
+    // Copies from pageable host memory are staged before cudaMemcpyAsync
+    // returns (CUDA runtime API, "API synchronization behavior"), so the host
+    // tables and parameters may change right after each call.
+    cudaError_t e = cudaSuccess;
+    if (!table.empty())
+        e = cudaMemcpyAsync(b->d_views, table.data(), sizeof(WfView) * table.size(), cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "views upload");
     uint32_t want = b->opts.capacity ? b->opts.capacity : kDefaultCapacity;
     want = std::min<uint32_t>(std::max<uint32_t>(want, 32), kMaxCapacity);
-    rc = alloc_pool(b, want);
+    int rc = alloc_pool(b, want);
     if (rc != SOL_GPU_OK) return rc;
     rc = configure_launch(b);
     if (rc != SOL_GPU_OK) return rc;
     WfParams& h = b->host;
-    h.capacity = (uint32_t)std::min<uint64_t>(want, std::max<uint64_t>(pixels, 32));
     h.sort_threshold = b->opts.sort_threshold;
     h.refill_below = kWfRefillBelow;
-    h.num_views = n;
-    h.total_items = total_items;
-    {
-        // Bound on bounce iterations: every sample of every pixel, each vertex plus its start.
-        unsigned long long work = 0;
-        for (uint32_t i = 0; i < n; ++i)
-            work += (unsigned long long)views[i].width * views[i].height * ((unsigned long long)views[i].sample_count + 1ull);
-        h.max_iterations = work * ((unsigned long long)config->max_path_len + 2ull) + 16ull;
-    }
     h.cfg = to_config(*config);
-    h.views = b->d_views;
-    h.scenes = b->d_scenes;
     h.ctr = b->d_ctr;
-    cudaError_t e = cudaMemcpyAsync(b->d_params, &h, sizeof(WfParams), cudaMemcpyHostToDevice, stream);
-    if (e != cudaSuccess) return cuda_fail(e, "params upload");
     cudaEventRecord(b->ev_start, stream);
-    e = launch_wf_init(b->d_params, h.capacity, stream);
-    if (e != cudaSuccess) return cuda_fail(e, "wavefront init");
-    if (n > 0 && !b->opts.host_loop && build_graph(b) == SOL_GPU_OK) {
-        e = cudaGraphLaunch(b->exec, stream);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
-    } else if (n > 0) {
-        // Host-driven loop: the same stages, one iteration per round trip.
-        cudaGraphConditionalHandle none{};
-        for (uint64_t it = 0;; ++it) {
-            e = launch_wf_iteration(b->d_params, b->launch, none, 0, stream);
-            if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_ctr, b->d_ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-            if (e != cudaSuccess) return cuda_fail(e, "wavefront iteration");
-            if (!b->h_ctr->more) break;
-            if (it > h.max_iterations) return fail(SOL_GPU_ERR_TIMEOUT, "bounce loop exceeded its bound");
+    for (const WfPass& pass : passes) {
+        if (pass.num_views == 0) continue;
+        h.capacity = (uint32_t)std::min<uint64_t>(want, std::max<uint64_t>(pass.total_items, 32));
+        h.num_views = pass.num_views;
+        h.total_items = pass.total_items;
+        h.views = b->d_views + pass.first_view;
+        // Bound on bounce iterations: a path takes at most max_path_len + 1
+        // of them (its start and each vertex) and a slot runs its paths one
+        // after the other, so no render of these items needs more than
+        // items x (max_path_len + 2).
+        h.max_iterations = b->max_iterations ? b->max_iterations
+                                             : (unsigned long long)pass.total_items * (config->max_path_len + 2ull) + 16ull;
+        e = cudaMemcpyAsync(b->d_params, &h, sizeof(WfParams), cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "params upload");
+        e = launch_wf_init(b->d_params, h.capacity, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "wavefront init");
+        if (!b->opts.host_loop && build_graph(b) == SOL_GPU_OK) {
+            e = cudaGraphLaunch(b->exec, stream);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+        } else {
+            // Host-driven loop: the same stages, one iteration per round trip.
+            cudaGraphConditionalHandle none{};
+            for (uint64_t it = 0;; ++it) {
+                e = launch_wf_iteration(b->d_params, b->wf_table, b->basic, b->launch, none, 0, stream);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_ctr, b->d_ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+                if (e != cudaSuccess) return cuda_fail(e, "wavefront iteration");
+                if (!b->h_ctr->more) break;
+                if (it > h.max_iterations) return fail(SOL_GPU_ERR_TIMEOUT, "bounce loop exceeded its bound");
+            }
         }
+        e = launch_sum_samples_views(h.views, pass.num_views, pass.sum_floats, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "sum pass");
     }
     cudaEventRecord(b->ev_stop, stream);
     b->rendered = true;
     b->last_dc = false;
+    b->last_passes = (uint32_t)passes.size();
+    (void)paths;
     return SOL_GPU_OK;
+}
+
+int render_batch(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuView* views, uint32_t n, cudaStream_t stream) {
+    int rc = refresh_scenes(b);
+    if (rc != SOL_GPU_OK) return rc;
+    if (b->opts.schedule == SOL_GPU_BATCH_MEGAKERNEL) return render_megakernel(b, config, views, n, stream);
+    return render_wavefront(b, config, views, n, stream);
 }
 
 std::string device_name(int device) {
@@ -361,6 +524,8 @@ int sol_gpu_batch_create(SolGpuScene* const* scenes, uint32_t num_scenes, const 
     std::vector<SceneView> views(num_scenes);
     for (uint32_t i = 0; i < num_scenes; ++i) views[i] = scenes[i]->view;
     b->h_scenes = views;
+    for (uint32_t i = 0; i < num_scenes && i < kWfMaxScenes; ++i) b->wf_table.v[i] = views[i];
+    b->basic = std::all_of(b->scenes.begin(), b->scenes.end(), [](const SolGpuScene* s) { return s->basic_shading; });
     cudaError_t e = cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_params), sizeof(WfParams));
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_ctr), sizeof(WfCounters));
@@ -491,6 +656,11 @@ int sol_gpu_batch_stats(SolGpuBatch* b, SolGpuRenderStats* out) {
         out->paths = c.paths;
         out->rays = c.rays;
         out->shadow_rays = c.shadow_rays;
+        out->launches = b->last_passes;
+        if (c.error & kFaultPathLoop) {
+            for (SolGpuScene* sc : b->scenes) check_fault(sc);   // clear what the stopped render left
+            return fail(SOL_GPU_ERR_TIMEOUT, "the wavefront's bounce loop reached its iteration bound");
+        }
         if (c.error) return fail(SOL_GPU_ERR_BAD_INDEX, "a wavefront self-check failed (flags " + std::to_string(c.error) + ")");
     }
     float ms = 0.0f;
@@ -499,6 +669,18 @@ int sol_gpu_batch_stats(SolGpuBatch* b, SolGpuRenderStats* out) {
         int rc = check_fault(sc);
         if (rc != SOL_GPU_OK) return rc;
     }
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_batch_set_scratch_limit(SolGpuBatch* b, uint64_t bytes) {
+    if (!b) return fail(SOL_GPU_ERR_INVALID_ARG, "batch must not be NULL");
+    b->scratch_limit = bytes;
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_batch_set_iteration_limit(SolGpuBatch* b, uint64_t max_iterations) {
+    if (!b) return fail(SOL_GPU_ERR_INVALID_ARG, "batch must not be NULL");
+    b->max_iterations = max_iterations;
     return SOL_GPU_OK;
 }
 
@@ -530,7 +712,7 @@ int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const Sol
     size_t off = 0;
     for (auto& v : probe) { v.film = scratch + off; off += 3 * (size_t)v.width * v.height; v.sample_count = 1; }
     cudaStream_t s = b->capture;
-    const uint32_t caps[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21};
+    const uint32_t caps[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22};
     const uint32_t blocks[] = {64, 128, 256};
     const uint32_t sorts[] = {0u, 1u << 16, 0xffffffffu};
     float best_ms = 1e30f;

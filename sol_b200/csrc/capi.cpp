@@ -298,7 +298,8 @@ int sol_gpu_scene_create_ex(const SolGpuSceneDesc* desc, int device, uint32_t fl
     s->view.param_offsets = s->param_offsets;
     s->view.num_nodes = (uint32_t)flat.nodes.size();
     const size_t num_tris = gpu_bvh ? desc->num_triangles : flat.tris.size();
-    s->view.max_steps = (uint32_t)std::min<uint64_t>(2ull * (flat.nodes.size() + num_tris) + 16ull, 0xffffffffull);
+    s->default_max_steps = (uint32_t)std::min<uint64_t>(2ull * (flat.nodes.size() + num_tris) + 16ull, 0xffffffffull);
+    s->view.max_steps = s->default_max_steps;
     s->view.fault = s->fault;
     s->basic_shading =
         std::none_of(flat.textures.begin(), flat.textures.end(),
@@ -378,6 +379,12 @@ int sol_gpu_scene_set_schedule(SolGpuScene* scene, int schedule) {
 int sol_gpu_scene_set_scratch_limit(SolGpuScene* scene, uint64_t bytes) {
     if (!scene) return fail(SOL_GPU_ERR_INVALID_ARG, "scene must not be NULL");
     scene->scratch_limit = bytes;
+    return SOL_GPU_OK;
+}
+
+int sol_gpu_scene_set_traversal_limit(SolGpuScene* scene, uint32_t max_steps) {
+    if (!scene) return fail(SOL_GPU_ERR_INVALID_ARG, "scene must not be NULL");
+    scene->view.max_steps = max_steps ? max_steps : scene->default_max_steps;
     return SOL_GPU_OK;
 }
 

@@ -43,6 +43,7 @@ struct SolGpuScene {
     uint32_t last_chunk = 0;         // its samples per split chunk (0: per pixel)
     bool rendered = false;
     sol_b200::SceneView view{};
+    uint32_t default_max_steps = 0;  // traversal bound that no valid hierarchy reaches
     SolGpuSceneInfo info{};
     // Parameter vector (texture values), see sol_gpu_param_layout.
     std::vector<sol_b200::DTexture> host_textures;

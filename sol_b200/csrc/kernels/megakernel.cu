@@ -320,9 +320,11 @@ sum_samples(const float* __restrict__ scratch, uint32_t sample_count, size_t pla
     }
 }
 
-/// The sum pass of the split views of K1b: every float of those views' films
-/// (laid end to end from WfView::sum_begin) gets its pixel's per-sample colours
-/// added in sample order, starting from 0.
+/// The sum pass of split views (K1b's, the wavefront's): every float of those
+/// views' films (laid end to end from WfView::sum_begin) gets its pixel's
+/// per-sample colours added in sample order, starting from 0 -- or, for a
+/// chunk of a view's samples after the first, from the sum the earlier chunks
+/// left in `running`; the last chunk adds the sum into the film.
 __global__ void __launch_bounds__(256)
 sum_samples_views(const WfView* __restrict__ views, uint32_t num_views, uint64_t total) {
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total; g += (uint64_t)gridDim.x * blockDim.x) {
@@ -334,9 +336,10 @@ sum_samples_views(const WfView* __restrict__ views, uint32_t num_views, uint64_t
         const WfView& V = views[lo];
         const size_t n = 3 * (size_t)V.width * V.height;
         const size_t i = (size_t)(g - V.sum_begin);
-        float sum = 0.0f;
+        float sum = V.first_chunk ? 0.0f : V.running[i];
         for (uint32_t k = 0; k < V.sample_count; ++k) sum += V.scratch[(size_t)k * n + i];
-        V.film[i] += sum;
+        if (V.last_chunk) V.film[i] += sum;
+        else V.running[i] = sum;
     }
 }
 

@@ -1,27 +1,35 @@
 // K2-K6: batched wavefront path tracer for many views (cameras, films of uneven
 // size and sample count) over one or more scenes in a single launch sequence.
 //
-// A pool of C path slots lives in device memory (structure of arrays).  Each
-// bounce runs five stages over index queues:
-//   generate (K2): slots whose path ended add it to their pixel's sum; a pixel
-//                  that has run all its samples is written to its view's film
-//                  and the slot claims the next pixel of any view; the slot then
-//                  starts its pixel's next sample (camera ray).
-//   extend   (K3): closest-hit traversal of the queued rays; hits are binned by
-//                  the BSDF kind of the hit triangle (K6), misses end the path.
-//                  Persistent warps fetch rays lane by lane: when fewer than
-//                  `refill_below` lanes of a warp are still traversing, the warp
-//                  pauses, gives its idle lanes new rays and resumes.
+// Work items are (view, sample, pixel) triples, taken sample-major in 8x4
+// pixel tiles as the megakernel's split schedule takes them; a pool of C path
+// slots holds the paths in flight.  Each bounce runs five stages:
+//   generate (K2): every slot whose path ended writes the path's colour to its
+//                  view's per-sample scratch, claims the next work item and
+//                  starts its camera ray (path regeneration, so the pool stays
+//                  full until the items run out).
+//   extend   (K3): closest-hit traversal of the queued rays.  Rays travel in
+//                  the queue by value, so the stage reads its rays and writes
+//                  its hits in queue order; hits may be binned by the BSDF kind
+//                  of the hit triangle (K6).  Persistent warps fetch rays lane
+//                  by lane: when fewer than `refill_below` lanes of a warp are
+//                  still traversing, the warp pauses, gives its idle lanes new
+//                  rays and resumes.
 //   shade    (K5): SoL's per-vertex step (emission MIS, light sample, Russian
-//                  roulette, BSDF bounce) over the bins, kind by kind.
-//   shadow   (K4): any-hit traversal of the light samples' shadow rays.
+//                  roulette, BSDF bounce) per queue position, or per bin; the
+//                  next ray goes to the other parity's extend queue and the
+//                  light sample's shadow ray to the shadow queue.
+//   shadow   (K4): any-hit traversal of the shadow rays; an unoccluded light
+//                  sample adds its contribution to the path's colour.
 //   advance      : resets the consumed queues and decides whether to loop.
 // Queue appends are warp-aggregated (one atomic per distinct target per warp).
 // The five stages form the body of a CUDA graph WHILE node whose condition the
 // advance kernel sets, so a whole batch renders in one graph launch.
 //
-// A slot runs all samples of its pixel in order, so every pixel's sum is formed
-// in SoL's sample order and the films are bit-identical to the megakernel's.
+// Every path computes what the megakernel computes for it, in the same order
+// (the shadow stage runs before the next vertex's emission is added), and the
+// sum pass adds each pixel's colours in sample order starting from 0, so films
+// are bit-identical to the megakernel's.
 #include <cuda_runtime.h>
 
 #include "kernels.h"
@@ -57,10 +65,7 @@ __device__ __forceinline__ uint32_t append_keyed(uint32_t* counters, int key) {
     return __shfl_sync(mask, base, leader) + rank;
 }
 
-__device__ __forceinline__ uint32_t claim(uint32_t* counter) { return append(counter); }
-
-/// Sum over the whole warp; every lane of the block must call it (the stage
-/// kernels have no early exits, so all lanes reach their final reduction).
+/// Sum over the whole warp; every lane of the warp must call it.
 __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
     __syncwarp();
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
@@ -82,110 +87,87 @@ __device__ __forceinline__ DCamera view_camera(const WfView& v) {
     return c;
 }
 
-__device__ __forceinline__ void load_path(const WfParams& P, uint32_t slot, PathState& ps) {
-    const float4 o = P.ray_o[slot], d = P.ray_d[slot], t = P.thru[slot], c = P.color[slot];
-    ps.org = vec3(o.x, o.y, o.z);
-    ps.tmin = o.w;
-    ps.dir = vec3(d.x, d.y, d.z);
-    ps.pdf_prev = d.w;
-    ps.T = rgb(t.x, t.y, t.z);
-    ps.path_len = __float_as_uint(t.w);
-    ps.color = rgb(c.x, c.y, c.z);
-    ps.rng.state = P.rng[slot];
-}
-
-__device__ __forceinline__ void store_path(const WfParams& P, uint32_t slot, const PathState& ps) {
-    P.ray_o[slot] = make_float4(ps.org.x, ps.org.y, ps.org.z, ps.tmin);
-    P.ray_d[slot] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, ps.pdf_prev);
-    P.thru[slot] = make_float4(ps.T.r, ps.T.g, ps.T.b, __uint_as_float(ps.path_len));
-    P.color[slot] = make_float4(ps.color.r, ps.color.g, ps.color.b, 0.0f);
-    P.rng[slot] = ps.rng.state;
+__device__ __forceinline__ float tag_bits(uint32_t slot, uint32_t scene) {
+    return __uint_as_float(slot | (scene << kWfSlotBits));
 }
 
 __global__ void __launch_bounds__(256) wf_init(const WfParams* __restrict__ Pp) {
     const WfParams& P = *Pp;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.capacity; i += gridDim.x * blockDim.x) {
-        P.q_regen[0][i] = i;
+        P.q_ended[0][i] = i;
         P.pix[i] = make_uint4(kIdle, 0, 0, 0);
-        P.color[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        P.sum[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         WfCounters* c = P.ctr;
-        c->regen[0] = P.capacity;
-        c->regen[1] = 0;
+        c->ended[0] = P.capacity;
+        c->ended[1] = 0;
         c->extend[0] = c->extend[1] = 0;
         for (int b = 0; b < kWfBins; ++b) c->bins[b] = 0;
         c->shadow = 0;
         c->fetch_extend = c->fetch_shadow = 0;
         c->next_item = 0;
         c->iter = 0;
+        c->more = 1;
         c->paths = c->rays = c->shadow_rays = 0;
         c->error = 0;
     }
 }
 
-/// K2: finish ended paths, write finished pixels, claim work, start samples.
+/// K2: ended paths write their colour to the scratch of their (view, sample);
+/// their slots claim the next work items and start the camera rays.
 __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ Pp) {
     const WfParams& P = *Pp;
     WfCounters* ctr = P.ctr;
     const uint32_t p = ctr->iter & 1u;
-    const uint32_t n = ctr->regen[p];
+    const uint32_t n = ctr->ended[p];
     const uint32_t total = P.total_items;
     unsigned long long paths = 0;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t i = base + threadIdx.x;
         if (i >= n) continue;
-        const uint32_t slot = P.q_regen[p][i];
+        const uint32_t slot = P.q_ended[p][i];
         uint4 px = P.pix[slot];
-        float4 s = P.sum[slot];
-        if (px.x != kIdle) {
-            const float4 c = P.color[slot];
-            s = make_float4(s.x + c.x, s.y + c.y, s.z + c.z, 0.0f);   // path_tracer.cpp:19
-            px.w += 1;
-        }
-        bool started = false;
+        float4 col = P.color[slot];
         uint32_t claims = 0;
-        while (!started) {
-            if (++claims > total + 2u) { atomicOr(&ctr->error, kFaultClaimLoop); break; }
+        while (true) {
             if (px.x != kIdle) {
+                // path_tracer.cpp:19 -- the pixel's sum is formed by the sum pass
                 const WfView& v = P.views[px.x];
-                if (px.w < v.sample_count) {
-                    PathState ps;
-                    start_path(ps, view_camera(v), v.sample_index + px.w, px.y, px.z, v.width, v.height);
-                    ++paths;
-                    if (P.cfg.max_path_len == 0) { px.w += 1; continue; }   // empty path: black
-                    store_path(P, slot, ps);
-                    started = true;
-                    break;
-                }
-                // image.h:54-60 accumulate into the view's film
                 const size_t plane = (size_t)v.width * v.height;
-                const size_t at = (size_t)px.z * v.width + px.y;
-                v.film[at] += s.x;
-                v.film[at + plane] += s.y;
-                v.film[at + 2 * plane] += s.z;
+                float* f = v.scratch + (size_t)px.w * 3u * plane + (size_t)px.z * v.width + px.y;
+                f[0] = col.x;
+                f[plane] = col.y;
+                f[2 * plane] = col.z;
                 px.x = kIdle;
             }
-            const uint32_t item = claim(&ctr->next_item);
+            if (++claims > total + 2u) { atomicOr(&ctr->error, kFaultClaimLoop); break; }
+            const uint32_t item = append(&ctr->next_item);
             if (item >= total) break;
             const uint32_t vi = find_view(P.views, P.num_views, item);
             const WfView& v = P.views[vi];
-            const uint32_t local = item - v.item_begin;
+            const uint32_t per_sample = v.tiles_x * ((v.height + 3u) / 4u) * 32u;
+            uint32_t local = item - v.item_begin;
+            const uint32_t k = local / per_sample;
+            local -= k * per_sample;
             const uint32_t tile = local >> 5, l = local & 31u;
             const uint32_t x = (tile % v.tiles_x) * 8u + (l & 7u);
             const uint32_t y = (tile / v.tiles_x) * 4u + (l >> 3);
-            if (x < v.width && y < v.height) {
-                px = make_uint4(vi, x, y, 0);
-                s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            }
+            if (x >= v.width || y >= v.height) continue;
+            PathState ps;
+            start_path(ps, view_camera(v), v.sample_index + k, x, y, v.width, v.height);
+            ++paths;
+            px = make_uint4(vi, x, y, k);
+            col = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (P.cfg.max_path_len == 0) continue;   // empty path: black, written above
+            P.thru[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            P.color[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
+            P.rng[slot] = ps.rng.state;
+            const uint32_t q = append(&ctr->extend[p]);
+            P.ray_o[p][q] = make_float4(ps.org.x, ps.org.y, ps.org.z, ps.tmin);
+            P.ray_d[p][q] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, tag_bits(slot, v.scene));
+            break;
         }
         P.pix[slot] = px;
-        P.sum[slot] = s;
-        if (started) {
-            P.color[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            P.q_extend[p][append(&ctr->extend[p])] = slot;
-        }
     }
     paths = warp_sum(paths);
     if (lane_id() == 0 && paths) atomicAdd(&ctr->paths, paths);
@@ -194,15 +176,16 @@ __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ 
 /// Persistent traversal of a ray queue with dynamic ray fetch: every lane keeps
 /// one ray; at the top of each round the warp claims queue entries for its idle
 /// lanes with one atomic, then traverses until the ray is done or the warp has
-/// fewer than `refill_below` busy lanes.  `fetch(i, tr, stack, slot, sv)` starts
-/// queue entry i; `finish(slot, tr)` consumes a finished ray.
+/// fewer than `refill_below` busy lanes.  `fetch(i, tr, stack) -> scene`
+/// starts queue entry i; `finish(i, tr)` consumes a finished ray.
 template <bool kAnyHit, class Fetch, class Finish>
-__device__ __forceinline__ void trace_queue(uint32_t n, uint32_t* fetch_counter, int refill_below, Fetch fetch,
-                                            Finish finish, unsigned long long& rays) {
+__device__ __forceinline__ void trace_queue(const WfSceneTable& scenes, uint32_t n, uint32_t* fetch_counter,
+                                            int refill_below, Fetch fetch, Finish finish,
+                                            unsigned long long& rays) {
     Traversal<kAnyHit, false, true> tr;
     LocalStack stack;
-    const SceneView* sv = nullptr;
-    uint32_t slot = 0;
+    const SceneView* sv = &scenes.v[0];
+    uint32_t at = 0;
     bool has = false;
     bool more = true;   // warp-uniform: the queue may still hold entries
     TraversalCounters tc{0u, 0u};
@@ -219,7 +202,8 @@ __device__ __forceinline__ void trace_queue(uint32_t n, uint32_t* fetch_counter,
                 if (!has) {
                     const uint32_t i = base + __popc(want & ((1u << lane_id()) - 1u));
                     if (i < n) {
-                        fetch(i, tr, stack, slot, sv);
+                        at = i;
+                        sv = &scenes.v[fetch(i, tr, stack)];
                         has = true;
                         ++rays;
                     }
@@ -230,109 +214,137 @@ __device__ __forceinline__ void trace_queue(uint32_t n, uint32_t* fetch_counter,
         // Once the queue is drained there is nothing to refill: run to the end.
         if (has && tr.run(sv->nodes, sv->tris, tc, sv->num_nodes, sv->num_tris, sv->max_steps, sv->fault, stack,
                           more ? refill_below : 0)) {
-            finish(slot, tr);
+            finish(at, tr);
             has = false;
         }
     }
 }
 
-/// K3: closest hit for every queued ray; hits binned by BSDF kind (K6), misses end.
-__global__ void __launch_bounds__(256, kWfTraceMinBlocks) wf_extend(const WfParams* __restrict__ Pp) {
+/// K3: closest hit for every queued ray, written in queue order; hits binned by
+/// BSDF kind (K6) when the queue is long enough.
+__global__ void __launch_bounds__(256, kWfTraceMinBlocks)
+wf_extend(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable scenes) {
     const WfParams& P = *Pp;
     WfCounters* ctr = P.ctr;
     const uint32_t p = ctr->iter & 1u;
     const uint32_t n = ctr->extend[p];
     const bool sort = n >= P.sort_threshold;
+    const float4* __restrict__ ro = P.ray_o[p];
+    const float4* __restrict__ rd = P.ray_d[p];
     unsigned long long rays = 0;
-    auto fetch = [&](uint32_t i, Traversal<false, false, true>& tr, LocalStack& stack, uint32_t& slot,
-                     const SceneView*& sv) {
-        slot = P.q_extend[p][i];
-        const float4 o = P.ray_o[slot], d = P.ray_d[slot];
-        sv = &P.scenes[P.views[P.pix[slot].x].scene];
-        tr.start(vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, kFloatMax, sv->num_tris > 0, stack);
+    auto fetch = [&](uint32_t i, Traversal<false, false, true>& tr, LocalStack& stack) -> uint32_t {
+        const float4 o = ro[i], d = rd[i];
+        const uint32_t scene = __float_as_uint(d.w) >> kWfSlotBits;
+        tr.start(vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, kFloatMax, scenes.v[scene].num_tris > 0, stack);
+        return scene;
     };
-    auto finish = [&](uint32_t slot, const Traversal<false, false, true>& tr) {
-        if (tr.hit < 0) {
-            P.q_regen[p ^ 1u][append(&ctr->regen[p ^ 1u])] = slot;
-        } else {
-            P.hit[slot] = make_float2(__int_as_float(tr.hit), tr.tmax);
+    auto finish = [&](uint32_t i, const Traversal<false, false, true>& tr) {
+        P.hit[i] = make_float2(__int_as_float(tr.hit), tr.tmax);
+        if (sort) {
             int kind = kWfBins - 1;
-            if (sort) {
-                const SceneView& sv = P.scenes[P.views[P.pix[slot].x].scene];
+            if (tr.hit >= 0) {
+                const SceneView& sv = scenes.v[__float_as_uint(rd[i].w) >> kWfSlotBits];
                 const int b = __ldg(&sv.tris[tr.hit].bsdf);
                 kind = b < 0 ? kWfBins - 1 : sv.bsdfs[b].kind;
             }
-            P.q_bins[(size_t)kind * P.capacity + append_keyed(ctr->bins, kind)] = slot;
+            P.q_bins[(size_t)kind * P.capacity + append_keyed(ctr->bins, kind)] = i;
         }
     };
-    trace_queue<false>(n, &ctr->fetch_extend, P.refill_below, fetch, finish, rays);
+    trace_queue<false>(scenes, n, &ctr->fetch_extend, P.refill_below, fetch, finish, rays);
     rays = warp_sum(rays);
     if (lane_id() == 0 && rays) atomicAdd(&ctr->rays, rays);
 }
 
-/// K5: SoL's per-vertex step over the BSDF bins, kind by kind.
-__global__ void __launch_bounds__(256) wf_shade(const WfParams* __restrict__ Pp) {
+/// K5: SoL's per-vertex step for every closest hit (kind by kind when binned).
+template <bool kBasic>
+__global__ void __launch_bounds__(256, 3)
+wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable scenes) {
     const WfParams& P = *Pp;
     WfCounters* ctr = P.ctr;
     const uint32_t p = ctr->iter & 1u;
+    const uint32_t q = p ^ 1u;
+    const uint32_t n = ctr->extend[p];
+    const bool sort = n >= P.sort_threshold;
     uint32_t counts[kWfBins];
-    uint32_t total = 0;
-    for (int b = 0; b < kWfBins; ++b) { counts[b] = ctr->bins[b]; total += counts[b]; }
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        uint32_t j = i;
-        int b = 0;
-        while (j >= counts[b]) { j -= counts[b]; ++b; }
-        const uint32_t slot = P.q_bins[(size_t)b * P.capacity + j];
+    for (int b = 0; b < kWfBins; ++b) counts[b] = sort ? ctr->bins[b] : 0u;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+        uint32_t i = idx;
+        if (sort) {
+            uint32_t j = idx;
+            int b = 0;
+            while (b < kWfBins - 1 && j >= counts[b]) { j -= counts[b]; ++b; }
+            i = P.q_bins[(size_t)b * P.capacity + j];
+        }
+        const float4 o = P.ray_o[p][i], d = P.ray_d[p][i];
+        const float2 h = P.hit[i];
+        const uint32_t tag = __float_as_uint(d.w);
+        const uint32_t slot = tag & kWfSlotMask;
+        const int tri = __float_as_int(h.x);
+        if (tri < 0) {   // path_tracer.cpp:43-44: no hit, the path ends
+            P.q_ended[q][append(&ctr->ended[q])] = slot;
+            continue;
+        }
+        const SceneView& sv = scenes.v[tag >> kWfSlotBits];
         PathState ps;
-        load_path(P, slot, ps);
-        const float2 h = P.hit[slot];
-        const SceneView& sv = P.scenes[P.views[P.pix[slot].x].scene];
+        const float4 t4 = P.thru[slot], c4 = P.color[slot];
+        ps.org = vec3(o.x, o.y, o.z);
+        ps.tmin = o.w;
+        ps.dir = vec3(d.x, d.y, d.z);
+        ps.T = rgb(t4.x, t4.y, t4.z);
+        ps.pdf_prev = t4.w;
+        ps.color = rgb(c4.x, c4.y, c4.z);
+        ps.path_len = __float_as_uint(c4.w);
+        ps.rng.state = P.rng[slot];
         VertexOut vo;
-        shade_vertex(sv, P.cfg, 1.0f / (float)sv.num_lights, __float_as_int(h.x), h.y, ps, vo);
+        shade_vertex<kBasic>(sv, P.cfg, 1.0f / (float)sv.num_lights, tri, h.y, ps, vo);
         bool end = vo.end;
         if (!end) {
             ++ps.path_len;
             end = ps.path_len >= P.cfg.max_path_len;
         }
-        store_path(P, slot, ps);
+        P.color[slot] = make_float4(ps.color.r, ps.color.g, ps.color.b, __uint_as_float(ps.path_len));
+        if (!end) {
+            P.thru[slot] = make_float4(ps.T.r, ps.T.g, ps.T.b, ps.pdf_prev);
+            P.rng[slot] = ps.rng.state;
+            const uint32_t j = append(&ctr->extend[q]);
+            P.ray_o[q][j] = make_float4(ps.org.x, ps.org.y, ps.org.z, ps.tmin);
+            P.ray_d[q][j] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, d.w);
+        }
         if (vo.has_shadow) {
-            P.sh_o[slot] = make_float4(vo.sh_org.x, vo.sh_org.y, vo.sh_org.z, 0.0f);
-            P.sh_d[slot] = make_float4(vo.sh_dir.x, vo.sh_dir.y, vo.sh_dir.z, 0.0f);
-            P.pending[slot] = make_float4(vo.pending.r, vo.pending.g, vo.pending.b, end ? 1.0f : 0.0f);
-            P.q_shadow[append(&ctr->shadow)] = slot;
+            const uint32_t j = append(&ctr->shadow);
+            P.sh_o[j] = make_float4(vo.sh_org.x, vo.sh_org.y, vo.sh_org.z, d.w);
+            P.sh_d[j] = make_float4(vo.sh_dir.x, vo.sh_dir.y, vo.sh_dir.z, end ? 1.0f : 0.0f);
+            P.sh_c[j] = make_float4(vo.pending.r, vo.pending.g, vo.pending.b, 0.0f);
         } else if (end) {
-            P.q_regen[p ^ 1u][append(&ctr->regen[p ^ 1u])] = slot;
-        } else {
-            P.q_extend[p ^ 1u][append(&ctr->extend[p ^ 1u])] = slot;
+            P.q_ended[q][append(&ctr->ended[q])] = slot;
         }
     }
 }
 
 /// K4: shadow rays; the light sample's contribution is added when unoccluded.
-__global__ void __launch_bounds__(256, kWfTraceMinBlocks) wf_shadow(const WfParams* __restrict__ Pp) {
+__global__ void __launch_bounds__(256, kWfTraceMinBlocks)
+wf_shadow(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable scenes) {
     const WfParams& P = *Pp;
     WfCounters* ctr = P.ctr;
-    const uint32_t p = ctr->iter & 1u;
+    const uint32_t q = (ctr->iter & 1u) ^ 1u;
     const uint32_t n = ctr->shadow;
     const float offset = P.cfg.ray_offset;
     unsigned long long rays = 0;
-    auto fetch = [&](uint32_t i, Traversal<true, false, true>& tr, LocalStack& stack, uint32_t& slot,
-                     const SceneView*& sv) {
-        slot = P.q_shadow[i];
-        const float4 o = P.sh_o[slot], d = P.sh_d[slot];
-        sv = &P.scenes[P.views[P.pix[slot].x].scene];
-        tr.start(vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), offset, 1.0f - offset, sv->num_tris > 0, stack);
+    auto fetch = [&](uint32_t i, Traversal<true, false, true>& tr, LocalStack& stack) -> uint32_t {
+        const float4 o = P.sh_o[i], d = P.sh_d[i];
+        const uint32_t scene = __float_as_uint(o.w) >> kWfSlotBits;
+        tr.start(vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), offset, 1.0f - offset, scenes.v[scene].num_tris > 0, stack);
+        return scene;
     };
-    auto finish = [&](uint32_t slot, const Traversal<true, false, true>& tr) {
-        const float4 pend = P.pending[slot];
+    auto finish = [&](uint32_t i, const Traversal<true, false, true>& tr) {
+        const uint32_t slot = __float_as_uint(P.sh_o[i].w) & kWfSlotMask;
         if (tr.hit < 0) {
-            const float4 c = P.color[slot];
-            P.color[slot] = make_float4(c.x + pend.x, c.y + pend.y, c.z + pend.z, 0.0f);
+            const float4 c = P.color[slot], a = P.sh_c[i];
+            P.color[slot] = make_float4(c.x + a.x, c.y + a.y, c.z + a.z, c.w);
         }
-        if (pend.w != 0.0f) P.q_regen[p ^ 1u][append(&ctr->regen[p ^ 1u])] = slot;
-        else P.q_extend[p ^ 1u][append(&ctr->extend[p ^ 1u])] = slot;
+        if (P.sh_d[i].w != 0.0f) P.q_ended[q][append(&ctr->ended[q])] = slot;
     };
-    trace_queue<true>(n, &ctr->fetch_shadow, P.refill_below, fetch, finish, rays);
+    trace_queue<true>(scenes, n, &ctr->fetch_shadow, P.refill_below, fetch, finish, rays);
     rays = warp_sum(rays);
     if (lane_id() == 0 && rays) { atomicAdd(&ctr->rays, rays); atomicAdd(&ctr->shadow_rays, rays); }
 }
@@ -343,12 +355,12 @@ __global__ void wf_advance(const WfParams* __restrict__ Pp, cudaGraphConditional
     WfCounters* c = P.ctr;
     const uint32_t p = c->iter & 1u;
     c->extend[p] = 0;
-    c->regen[p] = 0;
+    c->ended[p] = 0;
     for (int b = 0; b < kWfBins; ++b) c->bins[b] = 0;
     c->shadow = 0;
     c->fetch_extend = c->fetch_shadow = 0;
     c->iter += 1;
-    bool more = c->extend[p ^ 1u] + c->regen[p ^ 1u] > 0;
+    bool more = c->extend[p ^ 1u] + c->ended[p ^ 1u] > 0;
     if (more && c->iter >= P.max_iterations) { c->error |= kFaultPathLoop; more = false; }
     c->more = more ? 1u : 0u;
     if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
@@ -362,7 +374,7 @@ int wavefront_blocks_per_sm(int stage, int block) {
     switch (stage) {
         case 0: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_generate, block, 0); break;
         case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend, block, 0); break;
-        case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shade, block, 0); break;
+        case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shade<false>, block, 0); break;
         default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow, block, 0); break;
     }
     return e == cudaSuccess ? n : -1;
@@ -375,12 +387,13 @@ cudaError_t launch_wf_init(const WfParams* params, uint32_t capacity, cudaStream
     return cudaGetLastError();
 }
 
-cudaError_t launch_wf_iteration(const WfParams* params, const WfLaunch& L, cudaGraphConditionalHandle handle,
-                                int use_handle, cudaStream_t stream) {
+cudaError_t launch_wf_iteration(const WfParams* params, const WfSceneTable& scenes, bool basic, const WfLaunch& L,
+                                cudaGraphConditionalHandle handle, int use_handle, cudaStream_t stream) {
     wf_generate<<<L.grid[0], L.block[0], 0, stream>>>(params);
-    wf_extend<<<L.grid[1], L.block[1], 0, stream>>>(params);
-    wf_shade<<<L.grid[2], L.block[2], 0, stream>>>(params);
-    wf_shadow<<<L.grid[3], L.block[3], 0, stream>>>(params);
+    wf_extend<<<L.grid[1], L.block[1], 0, stream>>>(params, scenes);
+    if (basic) wf_shade<true><<<L.grid[2], L.block[2], 0, stream>>>(params, scenes);
+    else wf_shade<false><<<L.grid[2], L.block[2], 0, stream>>>(params, scenes);
+    wf_shadow<<<L.grid[3], L.block[3], 0, stream>>>(params, scenes);
     wf_advance<<<1, 1, 0, stream>>>(params, handle, use_handle);
     return cudaGetLastError();
 }

@@ -1,4 +1,4 @@
-// Device-side structures of the batched wavefront renderer (host and device).
+// Device-side structures of the batched renderers (host and device).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -8,8 +8,8 @@
 
 namespace sol_b200 {
 
-/// Hit bins: one per BSDF kind (SOL_GPU_BSDF_*), the last for hits without a BSDF
-/// (and for everything when binning is off).
+/// Hit bins: one per BSDF kind (SOL_GPU_BSDF_*), the last for misses and hits
+/// without a BSDF (and for everything when binning is off).
 constexpr int kWfBins = 6;
 
 #ifndef SOL_WF_REFILL_BELOW
@@ -21,32 +21,52 @@ constexpr int kWfBins = 6;
 constexpr int kWfRefillBelow = SOL_WF_REFILL_BELOW;
 
 #ifndef SOL_WF_TRACE_MIN_BLOCKS
-#define SOL_WF_TRACE_MIN_BLOCKS 5
+#define SOL_WF_TRACE_MIN_BLOCKS 6
 #endif
 /// Resident 256-thread blocks per SM the traversal stages' registers must allow.
 constexpr int kWfTraceMinBlocks = SOL_WF_TRACE_MIN_BLOCKS;
 
+/// Scenes one wavefront batch may hold: they travel with every stage launch as
+/// a kernel parameter, and a ray carries its scene's index in the bits above
+/// its slot number.
+constexpr uint32_t kWfMaxScenes = 64;
+constexpr uint32_t kWfSlotBits = 26;
+constexpr uint32_t kWfSlotMask = (1u << kWfSlotBits) - 1u;
+/// Largest pool (slots in flight) of the wavefront.
+constexpr uint32_t kWfMaxCapacity = 1u << kWfSlotBits;
+
+struct WfSceneTable {
+    SceneView v[kWfMaxScenes];
+};
+
 /// One view of a batch: a constructed camera, its film and sample range.
+/// Work items are 8x4 pixel tiles of 32 items each; split views (every
+/// wavefront view, and the multi-view megakernel's views of more than one
+/// sample) have one item per (sample, pixel), taken sample-major, and write
+/// each path's colour to `scratch` (sample_count x 3 planes); the sum pass then
+/// adds every pixel's colours in sample order.
 struct WfView {
     float eye[3], dir[3], right[3], up[3];
     uint32_t scene;          // index into the batch's scenes
     uint32_t width, height;
-    uint32_t sample_count;
-    uint64_t sample_index;
+    uint32_t sample_count;   // samples of this launch
+    uint64_t sample_index;   // first sample of this launch
     float* film;             // device film, 3 planes of width*height, +=
-    uint32_t item_begin;     // first work item of this view (8x4 pixel tiles, 32 items each)
+    uint32_t item_begin;     // first work item of this view
     uint32_t tiles_x;
-    // Multi-view megakernel only: split views have one work item per (sample,
-    // pixel) and write each sample's colour to `scratch` (sample_count x 3
-    // planes); `sum_begin` is the view's first float in the sum pass.
     uint32_t split;
     float* scratch;
-    uint64_t sum_begin;
+    uint64_t sum_begin;      // the view's first float in the sum pass
+    // Samples of a view rendered over several launches (the wavefront's sample
+    // chunks): the pixel sums carried from chunk to chunk, or null.
+    float* running;
+    uint32_t first_chunk;    // the sum starts from 0 (else from `running`)
+    uint32_t last_chunk;     // the sum goes into the film (else into `running`)
 };
 
 struct WfCounters {
-    uint32_t extend[2];
-    uint32_t regen[2];
+    uint32_t extend[2];      // rays queued for the closest-hit stage, by parity
+    uint32_t ended[2];       // slots whose path ended, by parity
     uint32_t bins[kWfBins];
     uint32_t shadow;
     uint32_t fetch_extend;   // rays taken from the extend / shadow queue by the traversal stages
@@ -60,6 +80,10 @@ struct WfCounters {
 
 /// Everything the stages read, in device memory at a fixed address so that a
 /// captured graph can be replayed for new batches.
+///
+/// Path state lives per slot; rays travel in queues by value (origin and
+/// direction, the slot and scene in the direction's w), so the traversal
+/// stages read their input and write their output in queue order.
 struct WfParams {
     uint32_t capacity;
     uint32_t sort_threshold;
@@ -69,23 +93,21 @@ struct WfParams {
     int refill_below;        // a traversal warp refills its idle lanes when fewer than this many are busy
     DConfig cfg;
     const WfView* views;
-    const SceneView* scenes;
     WfCounters* ctr;
-    float4* ray_o;       // org, tmin
-    float4* ray_d;       // dir, pdf_prev
-    float4* thru;        // throughput, path_len
-    float4* color;       // radiance of the current path
+    // per slot
+    float4* thru;            // throughput, pdf_prev
+    float4* color;           // radiance gathered so far, path_len (bits)
     unsigned long long* rng;
-    uint4* pix;          // view, x, y, sample number (view = 0xffffffff: idle)
-    float4* sum;         // the pixel's sum so far
-    float4* sh_o;
-    float4* sh_d;
-    float4* pending;     // light-sample contribution, w = 1 when the path ends after it
-    float2* hit;         // triangle slot (int bits), t
-    uint32_t* q_extend[2];
-    uint32_t* q_regen[2];
-    uint32_t* q_bins;    // kWfBins * capacity
-    uint32_t* q_shadow;
+    uint4* pix;              // view, x, y, sample number within the launch (view = idle: none)
+    // per queue position
+    float4* ray_o[2];        // extend queue by parity: origin, tmin
+    float4* ray_d[2];        //                         direction, slot | scene << kWfSlotBits (bits)
+    float2* hit;             // closest hit of extend position i: triangle slot (int bits, -1: miss), t
+    uint32_t* q_bins;        // kWfBins * capacity extend positions
+    float4* sh_o;            // shadow queue: origin, slot | scene << kWfSlotBits (bits)
+    float4* sh_d;            //               direction, 1 when the path ends after it
+    float4* sh_c;            //               unoccluded contribution
+    uint32_t* q_ended[2];    // ended slots by parity
 };
 
 /// Grid and block of each stage: generate, extend, shade, shadow.
@@ -96,7 +118,10 @@ struct WfLaunch {
 
 int wavefront_blocks_per_sm(int stage, int block);
 cudaError_t launch_wf_init(const WfParams* params, uint32_t capacity, cudaStream_t stream);
-cudaError_t launch_wf_iteration(const WfParams* params, const WfLaunch& launch, cudaGraphConditionalHandle handle,
-                                int use_handle, cudaStream_t stream);
+/// One bounce of the wavefront: generate, extend, shade, shadow, advance.
+/// `basic`: every scene has basic shading (shade's build without image
+/// textures and Interp BSDFs).
+cudaError_t launch_wf_iteration(const WfParams* params, const WfSceneTable& scenes, bool basic, const WfLaunch& launch,
+                                cudaGraphConditionalHandle handle, int use_handle, cudaStream_t stream);
 
 }  // namespace sol_b200

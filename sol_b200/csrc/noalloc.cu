@@ -22,6 +22,17 @@
 // it; the caller must order them.  The first call on a device looks the
 // array's device address up (cudaGetSymbolAddress); make that first call
 // before any stream capture.
+//
+// The tables are built on the host and reach the array as kernel parameters:
+// a small copy kernel takes up to 30 KiB of them by value per launch and
+// stores them, so no host-to-device copy from pageable memory is involved
+// (the launch itself snapshots its parameters).
+//
+// With lazy module loading (the CUDA 12 default) the library's device image,
+// and with it the array, becomes resident on a device at the library's first
+// launch there (with CUDA_MODULE_LOADING=EAGER, when the library is loaded).
+// The cached address is that of the current CUDA context of the device: after
+// cudaDeviceReset the library must not be used in the same process.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -48,6 +59,41 @@ static_assert(kNoAllocScratchBytes <= 64 * 1024, "scratch stays under 64 KiB");
 /// The scratch array itself.  In host code this name is only a stand-in for the
 /// device object; its device address comes from cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+/// One piece of the host-built scratch image, passed to the copy kernel by value.
+constexpr uint32_t kUploadChunkBytes = 30 * 1024;
+struct UploadChunk {
+    uint32_t offset;   // byte offset in the scratch array (multiple of 16)
+    uint32_t bytes;    // multiple of 16, at most kUploadChunkBytes
+    uint32_t pad[2];
+    uint4 data[kUploadChunkBytes / 16];
+};
+static_assert(sizeof(UploadChunk) <= 32764, "kernel parameters are limited to 32,764 bytes");
+
+/// Stores one chunk of the tables into the scratch array.
+__global__ void __launch_bounds__(256) upload_chunk(const __grid_constant__ UploadChunk c, unsigned char* dst) {
+    uint4* out = reinterpret_cast<uint4*>(dst + c.offset);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.bytes / 16; i += gridDim.x * blockDim.x)
+        out[i] = c.data[i];
+}
+
+/// Copies bytes [offset, offset + bytes) of the host image `src` (laid out as
+/// the scratch array) into the array at `dst`, one kernel launch per chunk.
+cudaError_t upload(const unsigned char* src, size_t offset, size_t bytes, unsigned char* dst, cudaStream_t stream) {
+    bytes = (bytes + 15) & ~(size_t)15;
+    UploadChunk c;
+    for (size_t at = 0; at < bytes; at += kUploadChunkBytes) {
+        const size_t n = bytes - at < kUploadChunkBytes ? bytes - at : kUploadChunkBytes;
+        c.offset = (uint32_t)(offset + at);
+        c.bytes = (uint32_t)n;
+        std::memcpy(c.data, src + offset + at, n);
+        const int blocks = (int)((n / 16 + 255) / 256);
+        upload_chunk<<<blocks, 256, 0, stream>>>(c, dst);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
@@ -91,11 +137,13 @@ extern "C" int sol_gpu_batch_forward_adjoint_noalloc(SolGpuScene* const* scenes,
         if (!scenes[i]) return fail(SOL_GPU_ERR_INVALID_ARG, "scene must not be NULL");
         if (scenes[i]->device != device) return fail(SOL_GPU_ERR_INVALID_ARG, "all scenes must be on one device");
     }
-    // The tables are built on the host stack (63 KB) and copied in; a copy from
-    // pageable memory is staged before cudaMemcpyAsync returns, so the stack may
-    // unwind afterwards.
-    SceneView scene_table[kNoAllocMaxScenes];
-    AdjView view_table[kNoAllocMaxViews];
+    // The tables are built on the host stack in the layout of the scratch array
+    // (63 KB, counters zero) and stored into it by upload(), whose launches take
+    // them by value: the stack may unwind as soon as this call returns.
+    alignas(16) unsigned char image[kNoAllocScratchBytes];
+    std::memset(image + kCountersOffset, 0, sizeof(DeviceCounters));
+    SceneView* scene_table = reinterpret_cast<SceneView*>(image + kScenesOffset);
+    AdjView* view_table = reinterpret_cast<AdjView*>(image + kViewsOffset);
     uint64_t items = 0;
     for (uint32_t i = 0; i < num_scenes; ++i) scene_table[i] = scenes[i]->view;
     for (uint32_t i = 0; i < num_views; ++i) {
@@ -130,9 +178,9 @@ extern "C" int sol_gpu_batch_forward_adjoint_noalloc(SolGpuScene* const* scenes,
     SceneView* d_scenes = reinterpret_cast<SceneView*>(scratch + kScenesOffset);
     AdjView* d_views = reinterpret_cast<AdjView*>(scratch + kViewsOffset);
     DeviceCounters* d_ctr = reinterpret_cast<DeviceCounters*>(scratch + kCountersOffset);
-    cudaError_t e = cudaMemcpyAsync(d_scenes, scene_table, sizeof(SceneView) * num_scenes, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_views, view_table, sizeof(AdjView) * num_views, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_ctr, 0, sizeof(DeviceCounters), st);
+    cudaError_t e = upload(image, kScenesOffset, sizeof(SceneView) * num_scenes, scratch, st);
+    if (e == cudaSuccess) e = upload(image, kViewsOffset, sizeof(AdjView) * num_views, scratch, st);
+    if (e == cudaSuccess) e = upload(image, kCountersOffset, sizeof(DeviceCounters), scratch, st);
     if (e != cudaSuccess) return cuda_fail(e, "scratch upload");
     int num_sms = 0;
     e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device);

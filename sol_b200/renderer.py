@@ -113,6 +113,11 @@ class GpuScene:
         """Bytes of split-schedule scratch a render may use (0: default); larger renders run in chunks."""
         capi.check(capi.lib.sol_gpu_scene_set_scratch_limit(self.handle, int(nbytes)), "sol_gpu_scene_set_scratch_limit")
 
+    def set_traversal_limit(self, max_steps: int) -> None:
+        """Self-check bound on one BVH traversal's loop steps (0: default); exceeding it fails the render."""
+        capi.check(capi.lib.sol_gpu_scene_set_traversal_limit(self.handle, int(max_steps)),
+                   "sol_gpu_scene_set_traversal_limit")
+
     def trace(self, rays_ptr: int, count: int, any_hit: bool, hits_ptr: int, stream: int = 0) -> None:
         """Device-pointer batch query (SolGpuRay in, SolGpuHit out)."""
         capi.check(capi.lib.sol_gpu_trace(self.handle, rays_ptr, count, int(any_hit), hits_ptr, stream), "sol_gpu_trace")
@@ -312,6 +317,15 @@ class BatchRenderer:
         out = capi.SolGpuRenderStats()
         capi.check(capi.lib.sol_gpu_batch_stats(self.handle, C.byref(out)), "sol_gpu_batch_stats")
         return out
+
+    def set_scratch_limit(self, nbytes: int) -> None:
+        """Wavefront scratch bytes per render (0: default); larger renders run in chunks of samples."""
+        capi.check(capi.lib.sol_gpu_batch_set_scratch_limit(self.handle, int(nbytes)), "sol_gpu_batch_set_scratch_limit")
+
+    def set_iteration_limit(self, max_iterations: int) -> None:
+        """Self-check bound on the wavefront's bounce-loop iterations (0: default)."""
+        capi.check(capi.lib.sol_gpu_batch_set_iteration_limit(self.handle, int(max_iterations)),
+                   "sol_gpu_batch_set_iteration_limit")
 
     def close(self) -> None:
         if getattr(self, "handle", None):

@@ -28,13 +28,15 @@ def _views(scene, n, seed, max_side=96, max_spp=6):
     return out
 
 
-def _render_both(scenes, specs, cfg, **opts):
+def _render_both(scenes, specs, cfg, scratch_limit=0, **opts):
     import torch
     from sol_b200.renderer import BatchRenderer, GpuPathTracer, GpuScene
     gscenes = [GpuScene(s) for s in scenes]
     films_b = [torch.full((3, h, w), 0.5, dtype=torch.float32, device="cuda") for (_, _, w, h, _, _) in specs]
     films_m = [f.clone() for f in films_b]
     br = BatchRenderer(gscenes, **opts)
+    if scratch_limit:
+        br.set_scratch_limit(scratch_limit)
     br.render(cfg, br.views([(si, cam, w, h, idx, spp, f.data_ptr()) for (si, cam, w, h, idx, spp), f in zip(specs, films_b)]),
               torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
@@ -47,7 +49,10 @@ def _render_both(scenes, specs, cfg, **opts):
 
 
 @pytest.mark.parametrize("opts", [dict(), dict(capacity=4096, block_size=64), dict(sort_threshold=0xFFFFFFFF),
-                                  dict(host_loop=True, block_size=256), dict(schedule=1)])
+                                  dict(sort_threshold=0), dict(capacity=32, block_size=128),
+                                  dict(host_loop=True, block_size=256), dict(schedule=1),
+                                  # scratch for about two samples of every view: the samples run in chunks
+                                  dict(scratch_limit=2 * 3 * 4 * 96 * 96 * 12)])
 def test_batch_equals_megakernel_cornell(built, opts):
     from sol_b200 import scenes
     scene = scenes.cornell_box(0)
@@ -116,3 +121,18 @@ def test_autotune_auto_chooses_a_schedule(built, tmp_path):
                                                                           torch.cuda.current_stream().cuda_stream)
         torch.cuda.synchronize()
         assert torch.equal(f, ref)
+
+
+def test_wavefront_sample_chunks_match_megakernel(built):
+    """Views of many samples under a scratch limit of a few samples: the
+    wavefront renders them in chunks, carrying each pixel's sum between chunks,
+    and the films keep the megakernel's bits."""
+    from sol_b200 import scenes
+    scene = scenes.cornell_box(2)
+    specs = [(0, scene.camera, 33, 17, 5, 13), (0, scene.camera, 8, 40, 0, 1), (0, scene.camera, 24, 24, 77, 7)]
+    limit = 4 * 3 * (33 * 17 + 8 * 40 + 24 * 24) * 3   # about three samples of each view, with running sums
+    b, m, st = _render_both([scene], specs, scenes.CORNELL_CONFIG, scratch_limit=limit)
+    assert st.launches > 1   # several sample chunks
+    for fb, fm in zip(b, m):
+        assert np.array_equal(fb, fm)
+    assert st.paths == sum(w * h * spp for (_, _, w, h, _, spp) in specs)

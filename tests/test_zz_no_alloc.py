@@ -3,7 +3,9 @@
 The allocation-free entry point runs the same fused forward + adjoint kernel
 with its tables and counters in a fixed array inside the library.  Two calls in
 a row must each give the films (bit for bit), losses and gradients of the
-batch entry point on the same views; oversized calls must be refused.
+batch entry point on the same views, and the second (after the first has set
+the device up) must leave the device's free memory unchanged; oversized calls
+must be refused.
 """
 import ctypes as C
 
@@ -72,11 +74,17 @@ def test_noalloc_matches_batch_entry_point_twice(built):
     outs = [_buffers(torch, views, counts) for _ in range(2)]
     arrays = [_adjoint_views(capi, views, f, targets, g, l) for (f, g, l) in outs]
     torch.cuda.synchronize()
+    free = []
     for arr in arrays:
+        before = torch.cuda.mem_get_info()[0]
         capi.check(capi.lib.sol_gpu_batch_forward_adjoint_noalloc(handles, 2, C.byref(c_cfg), arr, len(views),
                                                                   stream),
                    "sol_gpu_batch_forward_adjoint_noalloc")
-    torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        free.append((before, torch.cuda.mem_get_info()[0]))
+    # The first call may load the library's module on this device; the second
+    # finds everything in place and takes no device memory.
+    assert free[1][0] == free[1][1], free
     for films, grads, losses in outs:
         for f, r in zip(films, films_ref):
             assert torch.equal(f, r)
