@@ -47,11 +47,13 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--small", action="store_true", help="quick run on a reduced frame (not a bench number)")
-    p.add_argument("--workload", default="frame", choices=["frame", "views", "adjoint", "scenes"],
-                   help="frame: one large frame per render call (default); views: 64 uneven views of a "
-                        "4,194,314-triangle field, batched wavefront vs 64 plain launches; adjoint: path-replay "
-                        "adjoint vs forward on the textured Cornell box; scenes: fused forward + adjoint over 32 "
-                        "independent scenes")
+    p.add_argument("--workload", default="frame", choices=["frame", "cornell", "views", "adjoint", "scenes"],
+                   help="frame: one large frame per render call (default; the other configurations are added "
+                        "under `configs`); cornell: the Cornell box at 256^2 x 16 spp; views: 64 uneven views of a "
+                        "4,194,314-triangle field, batched vs 64 plain launches; adjoint: path-replay adjoint vs "
+                        "forward on the textured Cornell box; scenes: fused forward + adjoint over 32 independent "
+                        "scenes")
+    p.add_argument("--no-configs", action="store_true", help="frame only: skip the other configurations")
     return p.parse_args()
 
 
@@ -156,36 +158,7 @@ def make_workload(small: bool):
     return scene, scenes.SPHERES_CONFIG, w, h, spp
 
 
-def cpu_model() -> str:
-    """The host CPU's model name (first /proc/cpuinfo entry)."""
-    try:
-        for line in Path("/proc/cpuinfo").read_text().splitlines():
-            if line.startswith("model name"):
-                return line.split(":", 1)[1].strip()
-    except OSError:
-        pass
-    return "unknown"
-
-
-def cpu_renderer(scene, threads: int):
-    """SoL's own path tracer (oracle/_ref, which links nothing of this
-    library) on `threads` host threads, or the oracle restatement where SoL's
-    sources were not built; returns (kind, run(sample_index, spp, w, h, cfg) ->
-    seconds of the render call alone)."""
-    import oracle
-    if oracle.ref_available():
-        ref = oracle.RefScene(scene)
-
-        def run(index, spp, w, h, cfg):
-            _, ms = ref.render(cfg, w, h, spp, sample_index=index, threads=threads)
-            return ms / 1000.0
-        return "reference", run
-
-    def run_port(index, spp, w, h, cfg):
-        t = time.perf_counter()
-        oracle.render(scene, cfg, w, h, spp, sample_index=index, threads=threads)
-        return time.perf_counter() - t
-    return "port", run_port
+from bench_workloads import cpu_model, cpu_renderer  # noqa: E402  (one definition for every workload)
 
 
 def cpu_reference_mpaths(scene, cfg, w, h, target_s: float = 12.0, max_spp: int = 64):
@@ -193,9 +166,9 @@ def cpu_reference_mpaths(scene, cfg, w, h, target_s: float = 12.0, max_spp: int 
     then enough samples for about `target_s` seconds (paths are independent)."""
     threads = os.cpu_count() or 1
     kind, run = cpu_renderer(scene, threads)
-    t1 = run(0, 1, w, h, cfg)
+    _, t1 = run(0, 1, w, h, cfg)
     spp = int(min(max_spp, max(1, math.floor(target_s / max(t1, 1e-3)))))
-    t = run(1, spp, w, h, cfg) if spp > 1 else t1
+    t = run(1, spp, w, h, cfg)[1] if spp > 1 else t1
     paths = w * h * spp
     return {"value": paths / t / 1e6, "unit": METRIC, "cores": threads, "cpu_model": cpu_model(), "kind": kind,
             "sample": f"{spp} spp of the full {w}x{h} frame ({paths} paths) on {threads} threads, "
@@ -215,7 +188,7 @@ def run_reference(args):
     kind, run = cpu_renderer(scene, threads)
     for i in range(args.warmup):
         run(i * spp, spp, w, h, cfg)
-    times = [run((args.warmup + i) * spp, spp, w, h, cfg) for i in range(args.steps)]
+    times = [run((args.warmup + i) * spp, spp, w, h, cfg)[1] for i in range(args.steps)]
     total = sum(times)
     paths = w * h * spp * args.steps
     value = paths / total / 1e6
@@ -369,6 +342,12 @@ def run_ours(args):
                 line["cpu_baseline"] = cpu_reference_mpaths(scene, cfg, w, h)
             except Exception as e:   # reported, not fatal
                 line["cpu_baseline"] = {"value": None, "error": str(e)}
+        if world == 1 and not args.no_configs and not args.small:
+            # The other configurations, each with its own clocks, roofline and CPU baseline.
+            import bench_workloads
+            del gscene, pt, film, flush
+            torch.cuda.empty_cache()
+            line["configs"] = bench_workloads.sub_records(args, ClockSampler, load_peaks)
         print(json.dumps(line), flush=True)
     return 0
 

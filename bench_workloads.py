@@ -1,46 +1,100 @@
-"""The multi-view, adjoint and multi-scene measurements of bench.py (one GPU).
+"""The per-configuration measurements of bench.py (one GPU).
 
+  cornell  the Cornell box: 256x256, 16 spp, max path length 16, Russian
+           roulette from bounce 3, one megakernel render per step.
   views    64 seeded views (square side log-uniform 64-1024, 1-64 spp) of a
-           4,194,314-triangle sphere field (256 displaced spheres), rendered by
-           the batched wavefront in one call against 64 plain megakernel
-           launches.  Both give bit-identical films (same estimator, same
+           4,194,314-triangle sphere field (256 displaced spheres): the batched
+           renderer in one call (autotuned schedule), the wavefront and the
+           multi-view megakernel each on their own, against 64 plain megakernel
+           launches.  All give bit-identical films (same estimator, same
            seeds), so their RMSE is equal; it is reported against a 256-spp
            render of every view.
   adjoint  the textured Cornell box (two 256x256 RGB albedo images): forward
            render 128x128 x 16 spp, then the L2 loss against a 1024-spp target
            and the path-replay adjoint; the ratio adjoint / forward time is the
-           value.  The gradient is checked against central finite differences
-           (eps 1e-3, common random numbers) of the GPU forward on 64 seeded
-           parameters.
+           value.  The gradient is checked per parameter against central
+           finite differences (eps 1e-3, common random numbers) of the GPU
+           forward on 64 seeded parameters, and on 8 of them against central
+           differences of SoL's own CPU renderer.
   scenes   32 independent textured sphere fields (10k-2M triangles, films
            128^2-512^2, 16 spp): forward + L2 adjoint of all 32 in one fused
-           launch, against the forward alone; gradients checked per scene
-           against finite differences on 16 parameters.
+           launch, against the forward alone (batched and plain); gradients
+           checked per scene and per parameter against finite differences on
+           16 parameters.
 
 Every timed launch is preceded by a 256 MiB write that flushes L2, and timed
-with CUDA events on the launching stream.
+with CUDA events on the launching stream.  Each record carries the CPU
+baseline measured in the same run: SoL's own path tracer (oracle/_ref, which
+links nothing of this library) on the host's threads, on a stated sample of
+the same workload.
 """
 from __future__ import annotations
 
 import json
 import math
+import os
 import time
+from pathlib import Path
 
 import numpy as np
 
 METRIC = "Mpaths/s"
 EPS = 1e-3
+GRAD_REL_TOL = 0.02
 
+
+# ---------------------------------------------------------------------------
+# CPU reference (SoL's PathTracer)
+# ---------------------------------------------------------------------------
+
+def cpu_model() -> str:
+    """The host CPU's model name (first /proc/cpuinfo entry)."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_renderer(scene, threads: int, camera=None):
+    """SoL's own path tracer (oracle/_ref, which links nothing of this
+    library) on `threads` host threads, or the oracle restatement where SoL's
+    sources were not built; returns (kind, run(sample_index, spp, w, h, cfg) ->
+    (film, seconds of the render call alone))."""
+    import oracle
+    if oracle.ref_available():
+        ref = oracle.RefScene(scene, camera=camera)
+
+        def run(index, spp, w, h, cfg):
+            film, ms = ref.render(cfg, w, h, spp, sample_index=index, threads=threads)
+            return film, ms / 1000.0
+        run.ref = ref
+        return "reference", run
+
+    def run_port(index, spp, w, h, cfg):
+        t = time.perf_counter()
+        film = oracle.render(scene, cfg, w, h, spp, sample_index=index, threads=threads, camera=camera)
+        return film, time.perf_counter() - t
+    return "port", run_port
+
+
+def cpu_baseline(paths: float, seconds: float, kind: str, sample: str) -> dict:
+    threads = os.cpu_count() or 1
+    return {"value": paths / seconds / 1e6, "unit": METRIC, "cores": threads, "cpu_model": cpu_model(),
+            "kind": kind, "sample": sample}
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
 
 def _events(torch, n):
     return [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
 
 
-def _ms(evs):
-    return [a.elapsed_time(b) for a, b in evs]
-
-
-def _timed(torch, flush, stream, fn, steps, warmup, clocks=None):
+def _timed(torch, flush, stream, fn, steps, warmup):
     """Runs fn(i) warmup times, then steps times with an L2 flush before each;
     returns the per-step device times in ms."""
     for i in range(warmup):
@@ -53,180 +107,48 @@ def _timed(torch, flush, stream, fn, steps, warmup, clocks=None):
         fn(warmup + i)
         ev[i][1].record(stream)
     torch.cuda.synchronize()
-    return _ms(ev)
+    return [a.elapsed_time(b) for a, b in ev]
 
 
-def _rel_err(g, fd):
+def grad_check(g, fd, rel: float = GRAD_REL_TOL, floor_frac: float = 0.01) -> dict:
+    """Per-parameter comparison of adjoint gradients with finite differences.
+
+    A parameter passes when |g - fd| <= rel * max(|fd|, floor), where the
+    absolute floor is `floor_frac` of the largest |fd| in the checked set (the
+    finite difference of a float32 render carries rounding noise of that
+    order for parameters with almost no effect on the loss)."""
     g = np.asarray(g, np.float64)
     fd = np.asarray(fd, np.float64)
-    den = float(np.linalg.norm(fd))
-    return float(np.linalg.norm(g - fd) / den) if den > 0 else float(np.linalg.norm(g))
+    floor = floor_frac * float(np.max(np.abs(fd))) if fd.size else 0.0
+    scale = np.maximum(np.abs(fd), floor)
+    err = np.abs(g - fd) / np.where(scale > 0, scale, 1.0)
+    ok = err <= rel
+    worst = int(np.argmax(err)) if err.size else -1
+    return {"params": int(fd.size), "within_tol": int(np.sum(ok)), "tol_rel": rel, "abs_floor": floor,
+            "max_rel_err": float(np.max(err)) if err.size else 0.0,
+            "median_rel_err": float(np.median(err)) if err.size else 0.0,
+            "vector_rel_err": float(np.linalg.norm(g - fd) / max(np.linalg.norm(fd), 1e-30)),
+            "worst": None if worst < 0 else {"index": worst, "adjoint": float(g[worst]), "fd": float(fd[worst])}}
 
 
-def _fd_gradient(torch, gs, render_loss, indices):
-    """Central differences (eps 1e-3) of render_loss() over the given parameter indices."""
+def fd_gradient(gs, render_loss, indices, eps: float = EPS):
+    """Central differences of render_loss() over the given parameter indices."""
     base = gs.get_params()
     out = []
     for j in indices:
         v = base.copy()
-        v[j] = base[j] + EPS
+        v[j] = base[j] + eps
         gs.set_params(v)
         lp = render_loss()
-        v[j] = base[j] - EPS
+        v[j] = base[j] - eps
         gs.set_params(v)
         lm = render_loss()
-        out.append((lp - lm) / (2.0 * EPS))
+        out.append((lp - lm) / (2.0 * eps))
     gs.set_params(base)
     return np.asarray(out)
 
 
-def _common(args, metric, value, unit, ms, hib, config, clocks, launches, **extra):
-    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms, "higher_is_better": hib, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded procedural scenes)", "config": config, "gpu_launches": launches,
-            "clocks": clocks}
-    line.update(extra)
-    return line
-
-
-# ---------------------------------------------------------------------------
-# views: batched wavefront vs plain megakernel launches
-# ---------------------------------------------------------------------------
-
-def run_views(args, ClockSampler, load_peaks):
-    import torch
-    from sol_b200 import scenes
-    from sol_b200.renderer import BatchRenderer, GpuPathTracer, GpuScene
-    small = args.small
-    scene = scenes.sphere_field(16 if small else 256, seed=1)
-    views = scenes.view_set(8 if small else 64, seed=2, max_side=256 if small else 1024)
-    cfg = scenes.SPHERES_CONFIG
-    gs = GpuScene(scene)
-    info = gs.info()
-    stream = torch.cuda.current_stream()
-    sp = stream.cuda_stream
-    films = [torch.zeros((3, s, s), device="cuda") for _, s, _ in views]
-    tracers = [GpuPathTracer(gs, cfg, camera=cam) for cam, _, _ in views]
-    paths = float(sum(s * s * p for _, s, p in views))
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-
-    def plain(i):
-        for (cam, s, p), pt, f in zip(views, tracers, films):
-            pt.render_device(f.data_ptr(), s, s, i * 64, p, sp)
-
-    from sol_b200 import capi
-    br = BatchRenderer([gs], schedule=capi.BATCH_AUTO)        # autotuned: wavefront or multi-view megakernel
-    br_wf = BatchRenderer([gs], schedule=capi.BATCH_WAVEFRONT)
-
-    def varr(i, fl=None, r=None):
-        fl = fl or films
-        return (r or br).views([(0, cam, s, s, i * 64, p, f.data_ptr()) for (cam, s, p), f in zip(views, fl)])
-
-    t0 = time.perf_counter()
-    opts = br.autotune(cfg, varr(0))
-    tune_s = time.perf_counter() - t0
-    opts_wf = br_wf.autotune(cfg, varr(0, r=br_wf))
-    arrays = {i: varr(i) for i in range(args.warmup + args.steps)}
-    arrays_wf = {i: varr(i, r=br_wf) for i in range(args.warmup + args.steps)}
-
-    def batched(i):
-        br.render(cfg, arrays[i], sp)
-
-    def wavefront(i):
-        br_wf.render(cfg, arrays_wf[i], sp)
-
-    with ClockSampler(torch.cuda.current_device()) as clocks:
-        plain_ms = _timed(torch, flush, stream, plain, args.steps, args.warmup)
-        batch_ms = _timed(torch, flush, stream, batched, args.steps, args.warmup)
-        wf_ms = _timed(torch, flush, stream, wavefront, args.steps, args.warmup)
-    plain_s, batch_s, wf_s = sum(plain_ms) / 1000.0, sum(batch_ms) / 1000.0, sum(wf_ms) / 1000.0
-
-    # Same films from both schedules (one fresh render each).
-    fa = [torch.zeros_like(f) for f in films]
-    fb = [torch.zeros_like(f) for f in films]
-    for (cam, s, p), pt, f in zip(views, tracers, fa):
-        pt.render_device(f.data_ptr(), s, s, 0, p, sp)
-    br.render(cfg, varr(0, fb), sp)
-    fc = [torch.zeros_like(f) for f in films]
-    br_wf.render(cfg, varr(0, fc, br_wf), sp)
-    torch.cuda.synchronize()
-    identical = all(torch.equal(a, b) and torch.equal(a, c) for a, b, c in zip(fa, fb, fc))
-
-    # RMSE of each schedule's images against a 256-spp render of every view.
-    gt_spp = 256
-    rmse_a, rmse_b = [], []
-    for (cam, s, p), pt, a, b in zip(views, tracers, fa, fb):
-        g = torch.zeros_like(a)
-        pt.render_device(g.data_ptr(), s, s, 1 << 20, gt_spp, sp)
-        torch.cuda.synchronize()
-        g /= gt_spp
-        rmse_a.append(float(torch.sqrt(torch.mean((a / p - g) ** 2))))
-        rmse_b.append(float(torch.sqrt(torch.mean((b / p - g) ** 2))))
-
-    # Algorithmic bytes of the same rays (counting build of the megakernel, one view at a time).
-    gs.set_instrumented(True)
-    nodes = tris = rays = 0
-    for (cam, s, p), pt in zip(views, tracers):
-        tmp = torch.zeros((3, s, s), device="cuda")
-        pt.render_device(tmp.data_ptr(), s, s, 0, p, sp)
-        torch.cuda.synchronize()
-        st = pt.stats()
-        nodes, tris, rays = nodes + st.nodes_visited, tris + st.tris_tested, rays + st.rays
-    gs.set_instrumented(False)
-    alg = 64.0 * nodes + 48.0 * tris + 32.0 * rays
-
-    # End to end: view table built and uploaded, films read back to pinned host memory.
-    host = [torch.empty(f.shape, dtype=torch.float32, pin_memory=True) for f in films]
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for i in range(args.steps):
-        br.render(cfg, varr(100 + i), sp)
-        for h_, f in zip(host, films):
-            h_.copy_(f, non_blocking=True)
-        torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    peak, src = load_peaks()
-    achieved = alg / (batch_s / args.steps) / 1e9
-    import ctypes
-    cfgd = {"workload": f"{len(views)} uneven views (side log-U[64,{views and max(s for _, s, _ in views)}], "
-                        f"1-64 spp) of a {info.num_triangles}-triangle sphere field, batched (one call, autotuned "
-                        f"schedule) vs {len(views)} plain megakernel launches",
-            "triangles": info.num_triangles, "views": len(views), "paths_per_step": int(paths),
-            "pixels": int(sum(s * s for _, s, _ in views)), "max_path_len": cfg.max_path_len,
-            "l2": "flushed between steps (256 MiB write); scene larger than L2",
-            "batch_options": {"schedule": ["wavefront", "megakernel", "auto"][opts.schedule],
-                              "capacity": opts.capacity, "block_size": opts.block_size,
-                              "sort_threshold": opts.sort_threshold},
-            "wavefront_options": {"capacity": opts_wf.capacity, "block_size": opts_wf.block_size,
-                                  "sort_threshold": opts_wf.sort_threshold}, "small": bool(small)}
-    return _common(
-        args, METRIC, paths * args.steps / batch_s / 1e6, METRIC, 1000.0 * batch_s / args.steps, True, cfgd,
-        clocks.summary(), args.steps,
-        launch_note="per batched step: one call (one megakernel launch, or the wavefront's stage kernels in a CUDA "
-                    "graph); per plain step: one launch per view",
-        plain={"value": paths * args.steps / plain_s / 1e6, "unit": METRIC,
-               "ms_per_step": 1000.0 * plain_s / args.steps, "launches_per_step": len(views)},
-        speedup_vs_plain=plain_s / batch_s,
-        wavefront={"value": paths * args.steps / wf_s / 1e6, "unit": METRIC, "ms_per_step": 1000.0 * wf_s / args.steps,
-                   "speedup_vs_plain": plain_s / wf_s},
-        equal_rmse={"films_bit_identical": identical, "reference": f"{gt_spp}-spp megakernel render per view",
-                    "rmse_plain_mean": float(np.mean(rmse_a)), "rmse_batched_mean": float(np.mean(rmse_b))},
-        roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                  "traffic": None, "peak_source": src,
-                  "algorithmic_bytes_per_launch": alg},
-        e2e={"value": paths * args.steps / e2e_s / 1e6, "unit": METRIC,
-             "h2d_bytes_per_step": len(views) * ctypes.sizeof(capi.SolGpuView) + ctypes.sizeof(capi.SolGpuConfig),
-             "d2h_bytes_per_step": int(sum(f.numel() * 4 for f in films))},
-        autotune_s=tune_s,
-        scene={"triangles": info.num_triangles, "bvh_inner_nodes": info.num_nodes, "bvh_depth": info.bvh_depth,
-               "device_mb": info.device_bytes / 2**20, "build_ms": info.build_ms})
-
-
-# ---------------------------------------------------------------------------
-# adjoint: path-replay adjoint vs forward on the textured Cornell box
-# ---------------------------------------------------------------------------
-
-def _choose_params(gs, n, seed, scalars=False):
+def choose_params(gs, n, seed, scalars=False):
     """n seeded parameter indices: about an eighth from the constant colour
     textures (albedos, specular colours, emission) and, with `scalars`, the
     constant scalar textures; the rest texels."""
@@ -246,10 +168,237 @@ def _choose_params(gs, n, seed, scalars=False):
     return sorted(int(j) for j in pick)
 
 
-def run_adjoint(args, ClockSampler, load_peaks):
+def _base(args, metric, value, unit, ms, hib, config, clocks, launches, steps, warmup, **extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": steps, "warmup": warmup,
+            "ms_per_step": ms, "higher_is_better": hib, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scenes)", "config": config, "gpu_launches": launches,
+            "clocks": clocks}
+    line.update(extra)
+    return line
+
+
+def _alg_bytes(st, paths_split=0):
+    """Algorithmic bytes of a counted render: 64 B per BVH node, 48 B per
+    triangle, 32 B per ray, and 24 B per path of split-schedule colour scratch."""
+    return 64.0 * st.nodes_visited + 48.0 * st.tris_tested + 32.0 * st.rays + 24.0 * paths_split
+
+
+# ---------------------------------------------------------------------------
+# cornell: the reference's own configuration
+# ---------------------------------------------------------------------------
+
+def run_cornell(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=True):
+    import torch
+    from sol_b200 import scenes
+    from sol_b200.renderer import GpuPathTracer, GpuScene, Image
+    steps = steps or args.steps
+    warmup = warmup or args.warmup
+    scene, cfg, w, h, spp = scenes.cornell_frame()
+    gs = GpuScene(scene)
+    pt = GpuPathTracer(gs, cfg)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    film = torch.zeros((3, h, w), device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def render(i):
+        pt.render_device(film.data_ptr(), w, h, i * spp, spp, sp)
+
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        ms = _timed(torch, flush, stream, render, steps, warmup)
+    st = pt.stats()
+    gs.set_instrumented(True)
+    render(0)
+    torch.cuda.synchronize()
+    ist = pt.stats()
+    gs.set_instrumented(False)
+    paths = float(w * h * spp)
+    alg = _alg_bytes(ist, ist.paths if st.sample_chunk > 0 else 0)
+    mean_s = float(np.mean(ms)) / 1000.0
+    peak, src = load_peaks()
+    img = Image(w, h)
+    pt.render(img, 0, spp)
+    t0 = time.perf_counter()
+    for i in range(steps):
+        pt.render(img, (1 + i) * spp, spp)
+    e2e_s = (time.perf_counter() - t0) / steps
+    extra = {}
+    if cpu:
+        kind, run = cpu_renderer(scene, os.cpu_count() or 1)
+        run(0, 1, w, h, cfg)
+        _, t = run(0, spp, w, h, cfg)
+        extra["cpu_baseline"] = cpu_baseline(paths, t, kind, f"the whole {w}x{h} x {spp} spp render, one call")
+    import ctypes
+    from sol_b200 import capi
+    return _base(args, METRIC, paths / mean_s / 1e6, METRIC, mean_s * 1000.0, True,
+                 {"workload": f"Cornell box (36 triangles: room, light quad, glass and Phong boxes), {w}x{h}, "
+                              f"{spp} spp, max path length {cfg.max_path_len}, Russian roulette from bounce "
+                              f"{cfg.min_rr_path_len}", "width": w, "height": h, "spp": spp,
+                  "max_path_len": cfg.max_path_len, "l2": "flushed between steps (256 MiB write)"},
+                 clocks.summary(), steps * st.launches, steps, warmup,
+                 mrays_per_s=st.rays / mean_s / 1e6, rays_per_path=st.rays / paths,
+                 roofline={"bound": "hbm", "achieved": alg / mean_s / 1e9, "peak": peak, "unit": "GB/s",
+                           "frac": alg / mean_s / 1e9 / peak, "traffic": None, "peak_source": src,
+                           "algorithmic_bytes_per_launch": alg,
+                           "note": "36 triangles: the scene sits in L1/L2; launch-latency bound at 1M paths"},
+                 e2e={"value": paths / e2e_s / 1e6, "unit": METRIC,
+                      "h2d_bytes_per_step": ctypes.sizeof(capi.SolGpuCamera) + ctypes.sizeof(capi.SolGpuConfig) + 20,
+                      "d2h_bytes_per_step": 3 * w * h * 4}, **extra)
+
+
+# ---------------------------------------------------------------------------
+# views: batched renderer vs plain megakernel launches
+# ---------------------------------------------------------------------------
+
+def run_views(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=True):
+    import ctypes
+
+    import torch
+    from sol_b200 import capi, scenes
+    from sol_b200.renderer import BatchRenderer, GpuPathTracer, GpuScene
+    steps = steps or args.steps
+    warmup = warmup or args.warmup
+    small = args.small
+    scene = scenes.sphere_field(16 if small else 256, seed=1)
+    views = scenes.view_set(8 if small else 64, seed=2, max_side=256 if small else 1024)
+    cfg = scenes.SPHERES_CONFIG
+    gs = GpuScene(scene)
+    info = gs.info()
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    films = [torch.zeros((3, s, s), device="cuda") for _, s, _ in views]
+    tracers = [GpuPathTracer(gs, cfg, camera=cam) for cam, _, _ in views]
+    paths = float(sum(s * s * p for _, s, p in views))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def plain(i):
+        for (cam, s, p), pt, f in zip(views, tracers, films):
+            pt.render_device(f.data_ptr(), s, s, i * 64, p, sp)
+
+    renderers = {"batched": BatchRenderer([gs], schedule=capi.BATCH_AUTO),
+                 "wavefront": BatchRenderer([gs], schedule=capi.BATCH_WAVEFRONT),
+                 "megakernel": BatchRenderer([gs], schedule=capi.BATCH_MEGAKERNEL)}
+
+    def varr(r, i, fl=None):
+        fl = fl or films
+        return r.views([(0, cam, s, s, i * 64, p, f.data_ptr()) for (cam, s, p), f in zip(views, fl)])
+
+    tune = {}
+    for name, r in renderers.items():
+        t0 = time.perf_counter()
+        o = r.autotune(cfg, varr(r, 0))
+        tune[name] = {"schedule": ["wavefront", "megakernel", "auto"][o.schedule], "capacity": o.capacity,
+                      "block_size": o.block_size, "sort_threshold": o.sort_threshold,
+                      "seconds": time.perf_counter() - t0}
+    arrays = {name: {i: varr(r, i) for i in range(warmup + steps)} for name, r in renderers.items()}
+    times = {}
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        times["plain"] = _timed(torch, flush, stream, plain, steps, warmup)
+        for name, r in renderers.items():
+            times[name] = _timed(torch, flush, stream, lambda i, r=r, name=name: r.render(cfg, arrays[name][i], sp),
+                                 steps, warmup)
+    mean = {k: float(np.mean(v)) / 1000.0 for k, v in times.items()}
+    wf_stats = renderers["wavefront"].stats()
+
+    # Same films from every schedule (one fresh render each).
+    ref_films = [torch.zeros_like(f) for f in films]
+    for (cam, s, p), pt, f in zip(views, tracers, ref_films):
+        pt.render_device(f.data_ptr(), s, s, 0, p, sp)
+    identical = {}
+    for name, r in renderers.items():
+        fb = [torch.zeros_like(f) for f in films]
+        r.render(cfg, varr(r, 0, fb), sp)
+        torch.cuda.synchronize()
+        identical[name] = all(torch.equal(a, b) for a, b in zip(ref_films, fb))
+
+    # RMSE of the films against a 256-spp render of every view.
+    gt_spp = 16 if small else 256
+    rmse = []
+    for (cam, s, p), pt, a in zip(views, tracers, ref_films):
+        g = torch.zeros_like(a)
+        pt.render_device(g.data_ptr(), s, s, 1 << 20, gt_spp, sp)
+        torch.cuda.synchronize()
+        rmse.append(float(torch.sqrt(torch.mean((a / p - g / gt_spp) ** 2))))
+
+    # Algorithmic bytes of the same rays (counting build of the megakernel, one view at a time).
+    gs.set_instrumented(True)
+    nodes = tris = rays = 0
+    alg = 0.0
+    for (cam, s, p), pt in zip(views, tracers):
+        tmp = torch.zeros((3, s, s), device="cuda")
+        pt.render_device(tmp.data_ptr(), s, s, 0, p, sp)
+        torch.cuda.synchronize()
+        st = pt.stats()
+        alg += _alg_bytes(st, st.paths if st.sample_chunk > 0 else 0)
+    gs.set_instrumented(False)
+
+    # End to end through the batch entry point: view table built and uploaded,
+    # films read back to pinned host memory.
+    best = min(renderers, key=lambda k: mean[k])
+    r = renderers["batched"]
+    host = [torch.empty(f.shape, dtype=torch.float32, pin_memory=True) for f in films]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(steps):
+        r.render(cfg, varr(r, 100 + i), sp)
+        for h_, f in zip(host, films):
+            h_.copy_(f, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / steps
+
+    extra = {}
+    if cpu:
+        # SoL's PathTracer on every 16th view (4 views), up to 4 samples each.
+        kind = None
+        cpu_paths, cpu_s = 0.0, 0.0
+        sample_views = list(range(0, len(views), 16))
+        for k in sample_views:
+            cam, s, p = views[k]
+            kind, run = cpu_renderer(scene, os.cpu_count() or 1, camera=cam)
+            n = min(p, 4)
+            _, t = run(0, n, s, s, cfg)
+            cpu_paths += s * s * n
+            cpu_s += t
+        extra["cpu_baseline"] = cpu_baseline(cpu_paths, cpu_s, kind,
+                                             f"views {sample_views} at min(spp, 4) samples each "
+                                             f"({int(cpu_paths)} paths); scene build excluded")
+    peak, src = load_peaks()
+    value = paths / mean["batched"] / 1e6
+    cfgd = {"workload": f"{len(views)} uneven views (side log-U[64,1024], 1-64 spp) of a "
+                        f"{info.num_triangles}-triangle sphere field, batched in one call (autotuned schedule)",
+            "triangles": info.num_triangles, "views": len(views), "paths_per_step": int(paths),
+            "pixels": int(sum(s * s for _, s, _ in views)), "max_path_len": cfg.max_path_len,
+            "l2": "flushed between steps (256 MiB write); scene larger than L2", "small": bool(small)}
+    return _base(
+        args, METRIC, value, METRIC, 1000.0 * mean["batched"], True, cfgd, clocks.summary(), steps, steps, warmup,
+        launch_note="per batched step: one call (the wavefront's stage kernels in a CUDA graph, or one "
+                    "multi-view megakernel launch) plus the in-order sum pass; per plain step: one launch per view",
+        schedules={k: {"value": paths / v / 1e6, "unit": METRIC, "ms_per_step": 1000.0 * v,
+                       "vs_plain": mean["plain"] / v} for k, v in mean.items()},
+        autotune=tune, fastest=best,
+        wavefront_stats={"rays": wf_stats.rays, "shadow_rays": wf_stats.shadow_rays, "launches": wf_stats.launches},
+        equal_rmse={"films_bit_identical_to_plain": identical, "reference": f"{gt_spp}-spp megakernel render per view",
+                    "rmse_mean": float(np.mean(rmse)), "note": "identical films, so identical RMSE per schedule"},
+        roofline={"bound": "hbm", "achieved": alg / mean["batched"] / 1e9, "peak": peak, "unit": "GB/s",
+                  "frac": alg / mean["batched"] / 1e9 / peak, "traffic": None, "peak_source": src,
+                  "algorithmic_bytes_per_launch": alg},
+        e2e={"value": paths / e2e_s / 1e6, "unit": METRIC,
+             "h2d_bytes_per_step": len(views) * ctypes.sizeof(capi.SolGpuView) + ctypes.sizeof(capi.SolGpuConfig),
+             "d2h_bytes_per_step": int(sum(f.numel() * 4 for f in films))},
+        scene={"triangles": info.num_triangles, "bvh_inner_nodes": info.num_nodes, "bvh_depth": info.bvh_depth,
+               "device_mb": info.device_bytes / 2**20, "build_ms": info.build_ms}, **extra)
+
+
+# ---------------------------------------------------------------------------
+# adjoint: path-replay adjoint vs forward on the textured Cornell box
+# ---------------------------------------------------------------------------
+
+def run_adjoint(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=True):
     import torch
     from sol_b200 import scenes
     from sol_b200.renderer import BatchRenderer, GpuPathTracer, GpuScene, image_l2
+    steps = steps or args.steps
+    warmup = warmup or args.warmup
     W = H = 64 if args.small else 128
     SPP = 16
     tex = 64 if args.small else 256
@@ -261,7 +410,8 @@ def run_adjoint(args, ClockSampler, load_peaks):
     GpuPathTracer(truth, cfg).render_device(target.data_ptr(), W, H, 1 << 24, 1024, sp)
     torch.cuda.synchronize()
     target /= 1024
-    gs = GpuScene(scenes.cornell_box(0, textured=True, tex_size=tex, tex_seed=11))
+    scene = scenes.cornell_box(0, textured=True, tex_size=tex, tex_seed=11)
+    gs = GpuScene(scene)
     pt = GpuPathTracer(gs, cfg)
     count = gs.param_layout()[0]
     film = torch.zeros((3, H, W), device="cuda")
@@ -285,12 +435,12 @@ def run_adjoint(args, ClockSampler, load_peaks):
                                   grad.data_ptr(), loss.data_ptr())], sp)
 
     with ClockSampler(torch.cuda.current_device()) as clocks:
-        f_ms = _timed(torch, flush, stream, forward, args.steps, args.warmup)
-        a_ms = _timed(torch, flush, stream, adjoint, args.steps, args.warmup)
-        x_ms = _timed(torch, flush, stream, fused, args.steps, args.warmup)
+        f_ms = _timed(torch, flush, stream, forward, steps, warmup)
+        a_ms = _timed(torch, flush, stream, adjoint, steps, warmup)
+        x_ms = _timed(torch, flush, stream, fused, steps, warmup)
     fwd, adj, fus = np.mean(f_ms), np.mean(a_ms), np.mean(x_ms)
 
-    # Gradient check at one sample range against central differences of the GPU forward.
+    # Gradient at one sample range against central differences of the GPU forward.
     film.zero_()
     grad.zero_()
     loss.zero_()
@@ -298,39 +448,86 @@ def run_adjoint(args, ClockSampler, load_peaks):
     adjoint(7)
     torch.cuda.synchronize()
     g = grad.cpu().numpy()
+    tgt = target.double()
 
     def render_loss():
         f = torch.zeros((3, H, W), device="cuda")
         pt.render_device(f.data_ptr(), W, H, 7 * SPP, SPP, sp)
         torch.cuda.synchronize()
-        return float(((f.double() / SPP - target.double()) ** 2).sum())
+        return float(((f.double() / SPP - tgt) ** 2).sum())
 
-    idx = _choose_params(gs, 64, seed=5)
-    fd = _fd_gradient(torch, gs, render_loss, idx)
-    err = _rel_err(g[idx], fd)
-    # Paths are the unit for the time-per-path figures.
+    idx = choose_params(gs, 64, seed=5)
+    fd = fd_gradient(gs, render_loss, idx)
+    check = grad_check(g[idx], fd)
+    extra = {}
+    if cpu:
+        # SoL's renderer: its forward rate on the loss render, and central
+        # differences of its loss on 8 of the parameters (same sample range).
+        import oracle
+        tgt_np = target.cpu().numpy().astype(np.float64)
+        kind, run = cpu_renderer(scene, os.cpu_count() or 1)
+        _, t_fwd = run(7 * SPP, SPP, W, H, cfg)
+        sub = idx[::8]
+        base = gs.get_params()
+        fd_sol = []
+        t0 = time.perf_counter()
+        for j in sub:
+            vals = []
+            for sgn in (1.0, -1.0):
+                v = base.copy()
+                v[j] = base[j] + sgn * EPS
+                s2 = _with_params(scene, gs, v)
+                _, r2 = cpu_renderer(s2, os.cpu_count() or 1)
+                f, _ = r2(7 * SPP, SPP, W, H, cfg)
+                vals.append(float(((f.astype(np.float64) / SPP - tgt_np) ** 2).sum()))
+            fd_sol.append((vals[0] - vals[1]) / (2 * EPS))
+        fd_s = time.perf_counter() - t0
+        extra["cpu_baseline"] = cpu_baseline(W * H * SPP, t_fwd, kind, f"the forward loss render ({W}x{H} x {SPP} spp)")
+        extra["gradient_check_vs_sol_fd"] = dict(grad_check(g[sub], np.asarray(fd_sol)),
+                                                 cpu_fd_seconds_8_params=fd_s)
     paths = float(W * H * SPP)
     cfgd = {"workload": f"textured Cornell box ({tex}x{tex} RGB albedo images on back wall and floor), "
                         f"{W}x{H} x {SPP} spp loss render, max path length {cfg.max_path_len}",
             "params": count, "width": W, "height": H, "spp": SPP, "target_spp": 1024,
             "l2": "flushed between steps (256 MiB write)", "small": bool(args.small)}
-    return _common(
-        args, "PRB adjoint / forward time", adj / fwd, "ratio", adj, False, cfgd, clocks.summary(), 2 * args.steps,
-        forward_ms=fwd, adjoint_ms=adj, fused_ms=fus, fused_over_forward=fus / fwd,
+    return _base(
+        args, "PRB adjoint / forward time", adj / fwd, "ratio", adj, False, cfgd, clocks.summary(), 2 * steps,
+        steps, warmup, forward_ms=fwd, adjoint_ms=adj, fused_ms=fus, fused_over_forward=fus / fwd,
         forward_mpaths_s=paths / fwd / 1e3, adjoint_mpaths_s=paths / adj / 1e3,
-        gradient_check={"params": len(idx), "eps": EPS, "rel_err_vs_gpu_fd": err,
-                        "nonzero_fd": int(np.count_nonzero(fd))},
-        e2e={"value": adj / fwd, "unit": "ratio", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        gradient_check=dict(check, eps=EPS, nonzero_fd=int(np.count_nonzero(fd))),
+        e2e={"value": adj / fwd, "unit": "ratio", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}, **extra)
+
+
+def _with_params(scene, gs, values):
+    """A copy of `scene` whose textures hold the parameter vector `values`
+    (the layout of sol_gpu_param_layout: constants, then texel planes)."""
+    import copy
+    from sol_b200 import capi
+    _, tex_off, img_off = gs.param_layout()
+    s = copy.copy(scene)
+    s.textures = [copy.copy(t) for t in scene.textures]
+    s.images = [np.array(im, np.float32, copy=True) for im in scene.images]
+    for t, off in zip(s.textures, tex_off):
+        if t.type == capi.TEX_CONSTANT_COLOR:
+            t.value = tuple(float(x) for x in values[off:off + 3])
+        elif t.type == capi.TEX_CONSTANT:
+            t.value = (float(values[off]),) + tuple(t.value[1:])
+    for k, off in enumerate(img_off):
+        im = s.images[k]
+        s.images[k] = np.asarray(values[off:off + im.size], np.float32).reshape(im.shape)
+    return s
 
 
 # ---------------------------------------------------------------------------
 # scenes: fused forward + adjoint over 32 scenes in one launch
 # ---------------------------------------------------------------------------
 
-def run_scenes(args, ClockSampler, load_peaks):
+def run_scenes(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=True):
     import torch
-    from sol_b200 import scenes
+    from sol_b200 import capi, scenes
     from sol_b200.renderer import BatchRenderer, GpuPathTracer, GpuScene
+    steps = steps or args.steps
+    warmup = warmup or args.warmup
     SPP = 16
     num = 4 if args.small else 32
     t0 = time.perf_counter()
@@ -363,33 +560,30 @@ def run_scenes(args, ClockSampler, load_peaks):
     def fused(i):
         br.forward_adjoint(cfg, specs(i), sp)
 
-    def varr(i):
-        return br.views([(k, made[k][0].camera, s, s, i * SPP, SPP, films[k].data_ptr())
-                         for k, s in enumerate(sides)])
-    opts = br.autotune(cfg, varr(0))
-    arrays = {i: varr(i) for i in range(args.warmup + args.steps)}
-    from sol_b200 import capi
-    br_mk = BatchRenderer(gss, schedule=capi.BATCH_MEGAKERNEL)
-    arrays_mk = {i: br_mk.views([(k, made[k][0].camera, s, s, i * SPP, SPP, films[k].data_ptr())
-                                 for k, s in enumerate(sides)]) for i in range(args.warmup + args.steps)}
+    renderers = {"wavefront": BatchRenderer(gss, schedule=capi.BATCH_WAVEFRONT),
+                 "megakernel": BatchRenderer(gss, schedule=capi.BATCH_MEGAKERNEL)}
 
-    def batched(i):
-        br.render(cfg, arrays[i], sp)
-
-    def batched_mk(i):
-        br_mk.render(cfg, arrays_mk[i], sp)
+    def varr(r, i):
+        return r.views([(k, made[k][0].camera, s, s, i * SPP, SPP, films[k].data_ptr()) for k, s in enumerate(sides)])
+    tune = {}
+    for name, r in renderers.items():
+        o = r.autotune(cfg, varr(r, 0))
+        tune[name] = {"capacity": o.capacity, "block_size": o.block_size, "sort_threshold": o.sort_threshold}
+    arrays = {name: {i: varr(r, i) for i in range(warmup + steps)} for name, r in renderers.items()}
 
     def plain(i):
         for pt, s, f in zip(tracers, sides, films):
             pt.render_device(f.data_ptr(), s, s, i * SPP, SPP, sp)
 
+    times = {}
     with ClockSampler(torch.cuda.current_device()) as clocks:
-        x_ms = _timed(torch, flush, stream, fused, args.steps, args.warmup)
-        b_ms = _timed(torch, flush, stream, batched, args.steps, args.warmup)
-        m_ms = _timed(torch, flush, stream, batched_mk, args.steps, args.warmup)
-        p_ms = _timed(torch, flush, stream, plain, args.steps, args.warmup)
-    fus, bat, bmk, pla = np.mean(x_ms), np.mean(b_ms), np.mean(m_ms), np.mean(p_ms)
-    fwd = min(bat, bmk, pla)
+        times["fused"] = _timed(torch, flush, stream, fused, steps, warmup)
+        for name, r in renderers.items():
+            times[name] = _timed(torch, flush, stream, lambda i, r=r, name=name: r.render(cfg, arrays[name][i], sp),
+                                 steps, warmup)
+        times["plain"] = _timed(torch, flush, stream, plain, steps, warmup)
+    mean = {k: float(np.mean(v)) for k, v in times.items()}
+    fwd_batched = min(mean["wavefront"], mean["megakernel"])
 
     # Per-scene gradient check: 16 parameters against central differences of the forward.
     for f in films:
@@ -399,49 +593,78 @@ def run_scenes(args, ClockSampler, load_peaks):
     losses.zero_()
     fused(3)
     torch.cuda.synchronize()
-    errs = []
-    worst = None
+    checks = []
     for k, (gs, pt, s) in enumerate(zip(gss, tracers, sides)):
-        def render_loss(pt=pt, s=s, k=k):
+        tgt = targets[k].double()
+
+        def render_loss(pt=pt, s=s, tgt=tgt):
             f = torch.zeros((3, s, s), device="cuda")
             pt.render_device(f.data_ptr(), s, s, 3 * SPP, SPP, sp)
             torch.cuda.synchronize()
-            return float(((f.double() / SPP - targets[k].double()) ** 2).sum())
-        idx = _choose_params(gs, 16, seed=100 + k)
-        fd = _fd_gradient(torch, gs, render_loss, idx)
-        gk = grads[k].cpu().numpy()[idx]
-        errs.append(_rel_err(gk, fd))
-        if errs[-1] >= max(errs):
-            worst = {"scene": k, "params": idx, "adjoint": [float(f"{x:.5g}") for x in gk],
-                     "fd": [float(f"{x:.5g}") for x in fd]}
+            return float(((f.double() / SPP - tgt) ** 2).sum())
+        idx = choose_params(gs, 16, seed=100 + k)
+        fd = fd_gradient(gs, render_loss, idx)
+        checks.append(grad_check(grads[k].cpu().numpy()[idx], fd))
+    extra = {}
+    if cpu:
+        # SoL's PathTracer on scenes 0 and 1 at their full size and 16 spp.
+        cpu_paths, cpu_s, kind = 0.0, 0.0, None
+        for k in (0, 1):
+            kind, run = cpu_renderer(made[k][0], os.cpu_count() or 1)
+            _, t = run(0, SPP, sides[k], sides[k], cfg)
+            cpu_paths += sides[k] ** 2 * SPP
+            cpu_s += t
+        extra["cpu_baseline"] = cpu_baseline(cpu_paths, cpu_s, kind,
+                                             f"scenes 0 and 1 at {SPP} spp ({int(cpu_paths)} paths); scene build excluded")
     tris = [i.num_triangles for i in infos]
     cfgd = {"workload": f"{num} independent textured sphere fields ({min(tris)}-{max(tris)} triangles, "
                         f"{sum(tris)} in all), films {min(sides)}^2-{max(sides)}^2, {SPP} spp, fused forward + "
                         f"L2 path-replay adjoint in one launch",
             "scenes": num, "triangles_total": sum(tris), "paths_per_step": int(paths),
-            "max_path_len": cfg.max_path_len, "l2": "flushed between steps (256 MiB write)",
-            "batch_options": {"capacity": opts.capacity, "block_size": opts.block_size,
-                              "sort_threshold": opts.sort_threshold}, "small": bool(args.small)}
-    return _common(
-        args, METRIC, paths / fus / 1e3, METRIC, fus, True, cfgd, clocks.summary(), args.steps,
-        note="value: paths rendered and differentiated per second by the fused launch",
-        forward_ms={"batched_wavefront": bat, "batched_megakernel": bmk, "plain_megakernel_launches": pla},
-        fused_ms=fus, fused_over_forward=fus / fwd, adjoint_over_forward=(fus - fwd) / fwd,
-        gradient_check={"params_per_scene": 16, "eps": EPS, "rel_err_max": float(np.max(errs)),
-                        "rel_err_median": float(np.median(errs)),
-                        "scenes_within_2pct": int(np.sum(np.asarray(errs) <= 0.02)),
-                        "rel_err_per_scene": [float(f"{e:.3g}") for e in errs],
-                        "worst": worst},
-        e2e={"value": paths / fus / 1e3, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        scene_generation_s=gen_s, bvh_build_ms=float(sum(i.build_ms for i in infos)))
+            "max_path_len": cfg.max_path_len, "l2": "flushed between steps (256 MiB write)", "small": bool(args.small)}
+    return _base(
+        args, METRIC, paths / mean["fused"] / 1e3, METRIC, mean["fused"], True, cfgd, clocks.summary(), steps,
+        steps, warmup, note="value: paths rendered and differentiated per second by the fused launch",
+        forward={k: {"ms": mean[k], "value": paths / mean[k] / 1e3, "vs_plain": mean["plain"] / mean[k]}
+                 for k in ("wavefront", "megakernel", "plain")},
+        autotune=tune, fused_ms=mean["fused"], fused_over_forward=mean["fused"] / fwd_batched,
+        adjoint_over_forward=(mean["fused"] - fwd_batched) / fwd_batched,
+        gradient_check={"params_per_scene": 16, "eps": EPS, "tol_rel": GRAD_REL_TOL,
+                        "params_within_tol": int(sum(c["within_tol"] for c in checks)),
+                        "params_checked": int(sum(c["params"] for c in checks)),
+                        "scenes_all_within_tol": int(sum(c["within_tol"] == c["params"] for c in checks)),
+                        "max_rel_err_per_scene": [float(f"{c['max_rel_err']:.3g}") for c in checks],
+                        "worst_scene": int(np.argmax([c["max_rel_err"] for c in checks])),
+                        "worst": checks[int(np.argmax([c["max_rel_err"] for c in checks]))]["worst"]},
+        e2e={"value": paths / mean["fused"] / 1e3, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        scene_generation_s=gen_s, bvh_build_ms=float(sum(i.build_ms for i in infos)), **extra)
+
+
+RUNS = {"cornell": run_cornell, "views": run_views, "adjoint": run_adjoint, "scenes": run_scenes}
 
 
 def run(args, ClockSampler, load_peaks) -> int:
+    """One workload's full JSON line (bench.py --workload NAME)."""
     import torch
     from sol_b200 import build
     build.build()
     torch.cuda.set_device(0)
-    fn = {"views": run_views, "adjoint": run_adjoint, "scenes": run_scenes}[args.workload]
-    line = fn(args, ClockSampler, load_peaks)
+    line = RUNS[args.workload](args, ClockSampler, load_peaks)
     print(json.dumps(line), flush=True)
     return 0
+
+
+def sub_records(args, ClockSampler, load_peaks, steps: int = 5, warmup: int = 3) -> dict:
+    """Every other configuration, measured in the default bench run (fewer
+    steps each, so that the whole run stays within a few minutes); a record
+    that fails carries its error instead."""
+    out = {}
+    for name, fn in (("cornell", run_cornell), ("views", run_views), ("adjoint", run_adjoint),
+                     ("scenes", run_scenes)):
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn(args, ClockSampler, load_peaks, steps=steps, warmup=warmup, cpu=not args.no_cpu_baseline)
+        except Exception as e:   # reported in the line, not fatal to the headline
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["wall_s"] = time.perf_counter() - t0
+    return out

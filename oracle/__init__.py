@@ -115,6 +115,8 @@ def ref_lib() -> C.CDLL:
         lib.ref_scene_create.restype = C.c_void_p
         lib.ref_scene_destroy.argtypes = [C.c_void_p]
         lib.ref_scene_destroy.restype = None
+        lib.ref_scene_set_camera.argtypes = [C.c_void_p, C.POINTER(CameraArgs)]
+        lib.ref_scene_set_camera.restype = C.c_int
         lib.ref_scene_render.argtypes = [C.c_void_p, C.POINTER(capi.SolGpuConfig), C.c_uint64, C.c_uint32,
                                          C.c_uint32, C.c_uint32, f32p, f32p, f32p, C.c_int, C.POINTER(C.c_double)]
         lib.ref_scene_render.restype = C.c_int
@@ -237,6 +239,12 @@ class RefScene:
         if not rs.h:
             raise RuntimeError("sol::Scene::load failed: " + rs.lib.ref_last_error().decode())
         return rs
+
+    def set_camera(self, camera) -> None:
+        """Renders from now on through `camera` (a sol_b200.scene.Camera)."""
+        cam = camera_args(camera)
+        if self.lib.ref_scene_set_camera(self.h, C.byref(cam)) != 0:
+            raise RuntimeError("ref_scene_set_camera failed: " + self.lib.ref_last_error().decode())
 
     def counts(self) -> dict:
         """Sizes of the scene's light, BSDF, texture and image tables."""

@@ -142,6 +142,15 @@ RefScene* ref_scene_create(const SolGpuSceneDesc* d, const OracleCamera* cam) {
 
 void ref_scene_destroy(RefScene* s) { delete s; }
 
+/// Replaces the scene's camera (a new sol::PerspectiveCamera from the same
+/// constructor arguments), so one scene and its hierarchy serve many views.
+int ref_scene_set_camera(RefScene* rs, const OracleCamera* cam) {
+    if (!rs || !cam) { g_err = "null argument"; return -1; }
+    rs->scene.camera = std::make_unique<sol::PerspectiveCamera>(v3(cam->eye), v3(cam->dir), v3(cam->up), cam->fov,
+                                                                cam->aspect);
+    return 0;
+}
+
 /// A scene file loaded by SoL's own loader (sol::Scene::load, src/scene_loader.cpp:
 /// TOML scene description + OBJ/MTL import, src/formats/obj.cpp), with the
 /// camera's aspect ratio defaulting to `aspect_ratio` as test/driver.cpp:197-199

@@ -381,24 +381,38 @@ def view_set(num_views: int = 64, seed: int = 2, box: float = 10.0, min_side: in
     return out
 
 
-def scene_set(num_scenes: int = 32, seed: int = 4, min_tris: int = 10_000, max_tris: int = 2_000_000,
-              min_side: int = 128, max_side: int = 512, tex_size: int = 128):
-    """Independent textured sphere fields of uneven size: (Scene, side) per scene.
+def scene_set_plan(num_scenes: int = 32, seed: int = 4, min_tris: int = 10_000, max_tris: int = 2_000_000,
+                   min_side: int = 128, max_side: int = 512):
+    """The sizes scene_set draws: (spheres, segments, side) per scene.
 
     Per scene, in draw order from Pcg(seed): a triangle budget log-uniform in
     [min_tris, max_tris] and a square film side log-uniform in [min_side,
     max_side].  The budget is met with n = clamp(budget / 16384, 2, 128) spheres
     of seg^2 triangles each (seg segments, seg/2 + 1 bands), seg the even number
-    nearest sqrt(budget / n).  Every scene has its own tex_size^2 RGB albedo
-    image (ground and half of the diffuse spheres) and its own light emission.
-    """
+    nearest sqrt(budget / n)."""
     rng = Pcg(seed)
     out = []
-    for k in range(num_scenes):
+    for _ in range(num_scenes):
         budget = math.exp(rng.uniform(math.log(min_tris), math.log(max_tris)))
         side = int(round(math.exp(rng.uniform(math.log(min_side), math.log(max_side)))))
         n = max(2, min(128, int(round(budget / 16384))))
         seg = max(6, 2 * int(round(math.sqrt(budget / n) / 2)))
+        out.append((n, seg, side))
+    return out
+
+
+def scene_set(num_scenes: int = 32, seed: int = 4, min_tris: int = 10_000, max_tris: int = 2_000_000,
+              min_side: int = 128, max_side: int = 512, tex_size: int = 128, only=None):
+    """Independent textured sphere fields of uneven size (sizes from
+    scene_set_plan): (Scene, side) per scene.  Every scene has its own
+    tex_size^2 RGB albedo image (ground and half of the diffuse spheres) and
+    its own light emission.  `only`: indices of the scenes to build (scene k is
+    the same scene either way); they come back in index order.
+    """
+    out = []
+    for k, (n, seg, side) in enumerate(scene_set_plan(num_scenes, seed, min_tris, max_tris, min_side, max_side)):
+        if only is not None and k not in only:
+            continue
         sizes = [(seg // 2 + 1, seg)] * n
         out.append((sphere_field(n, seed=100 + k, textured=True, tex_size=tex_size, sphere_sizes=sizes,
                                  aspect=1.0), side))

@@ -1,0 +1,136 @@
+"""Parity on the benchmarked configurations themselves, against SoL's own
+PathTracer (oracle/_ref: SoL's sources, its BVH build and its renderer):
+
+  * the 1,048,586-triangle frame scene of the headline benchmark, the whole
+    1920x1080 frame at one sample per pixel;
+  * four of the 64 views of the 4,194,314-triangle views scene, through both
+    batch schedules (wavefront and multi-view megakernel);
+  * a scene of the 32-scene set through the fused forward + adjoint launch:
+    its film against SoL's, its gradient against central differences of
+    SoL's renderer;
+  * a converged Cornell box (1024 spp) against SoL's at the same samples, and
+    the Monte Carlo noise between disjoint sample ranges for scale.
+
+Per-pixel tolerance: 1e-4 relative (helpers.per_pixel_parity); in practice
+the films are bit-identical except where glibc's powf and the shared pow_
+of the Phong lobe round differently."""
+import numpy as np
+import pytest
+
+import oracle
+from helpers import per_pixel_parity
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not oracle.ref_available(), reason="SoL's sources were not built into oracle/_ref")]
+
+
+def test_frame_scene_full_frame_matches_sol(built):
+    from sol_b200 import scenes
+    from sol_b200.renderer import GpuPathTracer, Image
+    scene = scenes.sphere_field(64, seed=1)
+    cfg = scenes.SPHERES_CONFIG
+    assert scene.num_triangles == 1048586
+    cpu, _ = oracle.RefScene(scene).render(cfg, 1920, 1080, 1, sample_index=3)
+    img = Image(1920, 1080)
+    GpuPathTracer(scene, cfg).render(img, 3, 1)
+    exact, bad = per_pixel_parity(img.channels, cpu)
+    print(f"frame 1920x1080x1: {exact:.6f} of pixels bit-identical, {bad} above 1e-4")
+    assert bad == 0 and exact >= 0.999
+    assert float(cpu.mean()) > 0.01
+
+
+def test_views_scene_matches_sol_both_batch_schedules(built):
+    import torch
+    from sol_b200 import capi, scenes
+    from sol_b200.renderer import BatchRenderer, GpuScene
+    scene = scenes.sphere_field(256, seed=1)
+    cfg = scenes.SPHERES_CONFIG
+    assert scene.num_triangles == 4194314
+    views = scenes.view_set(64, seed=2)
+    pick = [0, 16, 32, 48]
+    ref = oracle.RefScene(scene)
+    expect = {}
+    for k in pick:
+        cam, side, _ = views[k]
+        ref.set_camera(cam)
+        expect[k], _ = ref.render(cfg, side, side, 1, sample_index=11 + k)
+    gs = GpuScene(scene)
+    for schedule in (capi.BATCH_WAVEFRONT, capi.BATCH_MEGAKERNEL):
+        br = BatchRenderer([gs], schedule=schedule)
+        films = {k: torch.zeros((3, views[k][1], views[k][1]), device="cuda") for k in pick}
+        br.render(cfg, br.views([(0, views[k][0], views[k][1], views[k][1], 11 + k, 1, films[k].data_ptr())
+                                 for k in pick]))
+        br.stats()
+        for k in pick:
+            exact, bad = per_pixel_parity(films[k].cpu().numpy(), expect[k])
+            print(f"schedule {schedule} view {k} ({views[k][1]}^2): {exact:.6f} bit-identical, {bad} above 1e-4")
+            assert bad == 0 and exact >= 0.999
+
+
+def test_scene_set_fused_forward_adjoint_matches_sol(built):
+    """The smallest scene of the 32-scene set (and its texture and emission
+    parameters) through sol_gpu_batch_forward_adjoint: the film equals SoL's
+    PathTracer's, and the gradient of the L2 loss matches central differences
+    of SoL's renderer's loss on 8 parameters (per parameter, 2 % with an
+    absolute floor of 1 % of the largest difference)."""
+    import torch
+    import bench_workloads as bw
+    from sol_b200 import scenes
+    from sol_b200.renderer import BatchRenderer, GpuPathTracer, GpuScene
+    plan = scenes.scene_set_plan()
+    k = min(range(len(plan)), key=lambda i: plan[i][0] * plan[i][1] ** 2)
+    (scene, side), = scenes.scene_set(only=[k])
+    side = min(side, 160)
+    cfg = scenes.SPHERES_CONFIG
+    SPP = 8
+    gs = GpuScene(scene)
+    target = torch.zeros((3, side, side), device="cuda")
+    GpuPathTracer(gs, cfg).render_device(target.data_ptr(), side, side, 1 << 22, 64)
+    target *= 0.9 / 64
+    film = torch.zeros_like(target)
+    grad = torch.zeros(gs.param_layout()[0], device="cuda")
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    BatchRenderer([gs]).forward_adjoint(cfg, [(0, scene.camera, side, side, 40, SPP, film.data_ptr(),
+                                               target.data_ptr(), grad.data_ptr(), loss.data_ptr())])
+    torch.cuda.synchronize()
+    cpu, _ = oracle.RefScene(scene).render(cfg, side, side, SPP, sample_index=40)
+    exact, bad = per_pixel_parity(film.cpu().numpy(), cpu)
+    assert bad == 0 and exact >= 0.999
+    tgt = target.cpu().numpy().astype(np.float64)
+    assert abs(float(loss.item()) - float(((cpu / SPP - tgt) ** 2).sum())) <= 1e-6 * float(loss.item()) + 1e-9
+    idx = bw.choose_params(gs, 8, seed=7)
+    base = gs.get_params()
+    fd = []
+    for j in idx:
+        vals = []
+        for sgn in (1.0, -1.0):
+            v = base.copy()
+            v[j] += sgn * bw.EPS
+            f, _ = oracle.RefScene(bw._with_params(scene, gs, v)).render(cfg, side, side, SPP, sample_index=40)
+            vals.append(float(((f.astype(np.float64) / SPP - tgt) ** 2).sum()))
+        fd.append((vals[0] - vals[1]) / (2 * bw.EPS))
+    check = bw.grad_check(grad.cpu().numpy()[idx], np.asarray(fd))
+    print("fused adjoint vs SoL FD:", check)
+    assert check["within_tol"] == check["params"]
+
+
+def test_converged_cornell_matches_sol(built):
+    """1024 samples per pixel of the 64x64 Cornell box: the GPU film and SoL's
+    at the same sample indices agree to RMSE <= 1e-6 of the mean (they are the
+    same estimator); two disjoint 1024-sample ranges differ by Monte Carlo
+    noise, reported for scale and bounded at 5 % of the mean."""
+    from sol_b200 import scenes
+    from sol_b200.renderer import GpuPathTracer, Image
+    scene, cfg, *_ = scenes.cornell_frame()
+    N = 1024
+    cpu, _ = oracle.RefScene(scene).render(cfg, 64, 64, N, sample_index=0)
+    pt = GpuPathTracer(scene, cfg)
+    a, b = Image(64, 64), Image(64, 64)
+    pt.render(a, 0, N)
+    pt.render(b, N, N)
+    mean = float(cpu.mean() / N)
+    rmse_same = float(np.sqrt(np.mean((a.channels / N - cpu / N) ** 2)))
+    rmse_noise = float(np.sqrt(np.mean((b.channels / N - cpu / N) ** 2)))
+    print(f"converged 64x64x{N}: mean {mean:.4f}, RMSE same samples {rmse_same:.3g}, disjoint samples {rmse_noise:.4f}")
+    assert rmse_same <= 1e-6 * mean
+    assert rmse_noise <= 0.05 * mean

@@ -145,3 +145,20 @@ def test_errors(tmp_path):
     (tmp_path / "c.toml").write_text('[camera]\ntype = "orthographic"\n')
     with pytest.raises(loader.SceneFormatError, match="Unknown camera type"):
         loader.load_scene(str(tmp_path / "c.toml"))
+
+
+@pytest.mark.parametrize("name", oracle.REFERENCE_SCENES)
+def test_stored_sol_scenes_render_like_sol(name):
+    """The stored scenes (tests/golden/sol_scenes) rendered by the CPU checker
+    match the film SoL's PathTracer made from its own load of the file."""
+    import sys
+    from pathlib import Path
+    golden = Path(__file__).resolve().parent / "golden"
+    sys.path.insert(0, str(golden))
+    import make_sol_scenes as fixtures
+    d = np.load(golden / "sol_scenes" / f"{name}.npz")
+    scene = fixtures.arrays_to_scene(d)
+    o = oracle.render(scene, fixtures.config(), fixtures.W, fixtures.H, fixtures.SPP, sample_index=fixtures.INDEX)
+    from helpers import per_pixel_parity
+    exact, bad = per_pixel_parity(o, d["film"])
+    assert bad == 0 and exact >= 0.99
