@@ -94,6 +94,21 @@ def load_peaks():
     return 6650.0, "fallback: MEASURED_PEAKS.json absent, 6.65 TB/s copy measured earlier on a B200"
 
 
+def l2_read_peak_gbs():
+    """L2 read bandwidth of this GPU in GB/s: 16-byte L1-bypassing loads over a
+    64 MiB buffer that L2 holds, 20 passes per launch, best of 5 launches
+    (sol_b200/csrc/probe.cu).  None where the probe library is missing."""
+    import ctypes
+    lib_path = ROOT / "sol_b200" / "lib" / "libsol_probe.so"
+    if not lib_path.exists():
+        return None
+    lib = ctypes.CDLL(str(lib_path))
+    lib.sol_probe_l2_read_gbs.restype = ctypes.c_double
+    lib.sol_probe_l2_read_gbs.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
+    v = lib.sol_probe_l2_read_gbs(64 << 20, 20, 5)
+    return v if v > 0 else None
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle sampling during the timed region."""
 
@@ -286,13 +301,18 @@ def run_ours(args):
     achieved = alg_bytes / (kernel_s / args.steps) / 1e9
     traffic = None
     measured = {}
+    captured_on = None
     tfile = ROOT / "profiles" / "megakernel_sphere_field_traffic.txt"
     if tfile.exists() and not args.small:
         for line in tfile.read_text().splitlines():
-            if ":" in line and not line.startswith("#"):
+            if line.startswith("# captured on commit:"):
+                captured_on = line.split(":", 1)[1].strip()
+            elif ":" in line and not line.startswith("#"):
                 key, val = line.split(":", 1)
                 measured[key.strip()] = float(val)
         traffic = measured.get("dram_bytes_per_launch")
+    l2_peak = l2_read_peak_gbs()
+    l2_achieved = measured.get("lts_bytes", 0.0) / (kernel_s / args.steps) / 1e9 if measured else None
     line = None
     if rank == 0:
         line = {
@@ -309,7 +329,8 @@ def run_ours(args):
                 "dram_read": measured.get("dram_bytes_read", 0.0) / ist.rays,
                 "dram_write": measured.get("dram_bytes_write", 0.0) / ist.rays,
                 "lts": measured.get("lts_bytes", 0.0) / ist.rays,
-                "source": "profiles/megakernel_sphere_field_traffic.txt (one-pass ncu capture of a full launch)"},
+                "source": "profiles/megakernel_sphere_field_traffic.txt (one-pass ncu capture of a full launch"
+                          + (f", build of commit {captured_on})" if captured_on else ")")},
             "achieved_gbs": None if not measured else {
                 "dram": (measured.get("dram_bytes_read", 0.0) + measured.get("dram_bytes_write", 0.0))
                         / (kernel_s / args.steps) / 1e9,
@@ -318,6 +339,10 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_src,
+                         "l2": None if not (l2_peak and l2_achieved) else {
+                             "achieved": l2_achieved, "peak": l2_peak, "unit": "GB/s", "frac": l2_achieved / l2_peak,
+                             "peak_source": "measured here: L2-resident 64 MiB read (sol_b200/csrc/probe.cu)",
+                             "bytes": "lts__t_bytes.sum of the stored one-pass ncu capture"},
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "note": "per render call (megakernel + in-order sum pass)" if st.sample_chunk > 0
                                  else "per render call (one megakernel launch)"},

@@ -33,8 +33,11 @@ struct LocalStack {
     __device__ __forceinline__ int get(int i) const { return v[i]; }
 };
 
+#ifndef SOL_SHARED_STACK_DEPTH
+#define SOL_SHARED_STACK_DEPTH 16
+#endif
 /// Entries of the traversal stack kept in shared memory by SharedStack.
-constexpr int kSharedStackDepth = 16;
+constexpr int kSharedStackDepth = SOL_SHARED_STACK_DEPTH;
 
 /// Traversal stack whose first kSharedStackDepth entries live in shared memory,
 /// laid out entry-major ([entry][thread] for kThreads threads, so a warp's
@@ -51,6 +54,22 @@ struct SharedStack {
     }
     __device__ __forceinline__ int get(int i) const {
         return i < kSharedStackDepth ? column[i * kThreads] : deep[i - kSharedStackDepth];
+    }
+};
+
+/// SharedStack with the thread stride given at run time (the block size), for
+/// kernels launched with several block sizes: `column` = a dynamic shared
+/// array of kSharedStackDepth * blockDim.x ints + threadIdx.x.
+struct SharedStackDyn {
+    int* column;
+    int stride;
+    int deep[kTraversalStack - kSharedStackDepth];
+    __device__ __forceinline__ void put(int i, int x) {
+        if (i < kSharedStackDepth) column[i * stride] = x;
+        else deep[i - kSharedStackDepth] = x;
+    }
+    __device__ __forceinline__ int get(int i) const {
+        return i < kSharedStackDepth ? column[i * stride] : deep[i - kSharedStackDepth];
     }
 };
 

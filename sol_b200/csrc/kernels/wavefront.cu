@@ -178,12 +178,24 @@ __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ 
 /// lanes with one atomic, then traverses until the ray is done or the warp has
 /// fewer than `refill_below` busy lanes.  `fetch(i, tr, stack) -> scene`
 /// starts queue entry i; `finish(i, tr)` consumes a finished ray.
+/// The traversal stack of a trace-stage lane (see kWfSharedStack).
+#if SOL_WF_SHARED_STACK
+using WfStack = SharedStackDyn;
+__device__ __forceinline__ WfStack make_stack() {
+    extern __shared__ int wf_stack_smem[];
+    return WfStack{wf_stack_smem + threadIdx.x, (int)blockDim.x, {}};
+}
+#else
+using WfStack = LocalStack;
+__device__ __forceinline__ WfStack make_stack() { return WfStack{}; }
+#endif
+
 template <bool kAnyHit, class Fetch, class Finish>
 __device__ __forceinline__ void trace_queue(const WfSceneTable& scenes, uint32_t n, uint32_t* fetch_counter,
                                             int refill_below, Fetch fetch, Finish finish,
                                             unsigned long long& rays) {
     Traversal<kAnyHit, false, true> tr;
-    LocalStack stack;
+    WfStack stack = make_stack();
     const SceneView* sv = &scenes.v[0];
     uint32_t at = 0;
     bool has = false;
@@ -232,7 +244,7 @@ wf_extend(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable 
     const float4* __restrict__ ro = P.ray_o[p];
     const float4* __restrict__ rd = P.ray_d[p];
     unsigned long long rays = 0;
-    auto fetch = [&](uint32_t i, Traversal<false, false, true>& tr, LocalStack& stack) -> uint32_t {
+    auto fetch = [&](uint32_t i, Traversal<false, false, true>& tr, WfStack& stack) -> uint32_t {
         const float4 o = ro[i], d = rd[i];
         const uint32_t scene = __float_as_uint(d.w) >> kWfSlotBits;
         tr.start(vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), o.w, kFloatMax, scenes.v[scene].num_tris > 0, stack);
@@ -330,7 +342,7 @@ wf_shadow(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable 
     const uint32_t n = ctr->shadow;
     const float offset = P.cfg.ray_offset;
     unsigned long long rays = 0;
-    auto fetch = [&](uint32_t i, Traversal<true, false, true>& tr, LocalStack& stack) -> uint32_t {
+    auto fetch = [&](uint32_t i, Traversal<true, false, true>& tr, WfStack& stack) -> uint32_t {
         const float4 o = P.sh_o[i], d = P.sh_d[i];
         const uint32_t scene = __float_as_uint(o.w) >> kWfSlotBits;
         tr.start(vec3(o.x, o.y, o.z), vec3(d.x, d.y, d.z), offset, 1.0f - offset, scenes.v[scene].num_tris > 0, stack);
@@ -366,16 +378,31 @@ __global__ void wf_advance(const WfParams* __restrict__ Pp, cudaGraphConditional
     if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
 }
 
+/// Dynamic shared memory of a traversal-stage block of `block` threads.
+size_t trace_smem(int block) { return kWfSharedStack ? sizeof(int) * kSharedStackDepth * (size_t)block : 0; }
+
+/// Lets the traversal stages use more than 48 KiB of dynamic shared memory
+/// (their stacks at 256 threads per block and kSharedStackDepth above 48), on
+/// the current device.
+cudaError_t allow_trace_smem() {
+    const int bytes = (int)trace_smem(256);
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(wf_extend, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(wf_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
+}
+
 }  // namespace
 
 int wavefront_blocks_per_sm(int stage, int block) {
     int n = 0;
+    if (allow_trace_smem() != cudaSuccess) return -1;
     cudaError_t e = cudaSuccess;
     switch (stage) {
         case 0: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_generate, block, 0); break;
-        case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend, block, 0); break;
+        case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend, block, trace_smem(block)); break;
         case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shade<false>, block, 0); break;
-        default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow, block, 0); break;
+        default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow, block, trace_smem(block)); break;
     }
     return e == cudaSuccess ? n : -1;
 }
@@ -390,10 +417,10 @@ cudaError_t launch_wf_init(const WfParams* params, uint32_t capacity, cudaStream
 cudaError_t launch_wf_iteration(const WfParams* params, const WfSceneTable& scenes, bool basic, const WfLaunch& L,
                                 cudaGraphConditionalHandle handle, int use_handle, cudaStream_t stream) {
     wf_generate<<<L.grid[0], L.block[0], 0, stream>>>(params);
-    wf_extend<<<L.grid[1], L.block[1], 0, stream>>>(params, scenes);
+    wf_extend<<<L.grid[1], L.block[1], trace_smem(L.block[1]), stream>>>(params, scenes);
     if (basic) wf_shade<true><<<L.grid[2], L.block[2], 0, stream>>>(params, scenes);
     else wf_shade<false><<<L.grid[2], L.block[2], 0, stream>>>(params, scenes);
-    wf_shadow<<<L.grid[3], L.block[3], 0, stream>>>(params, scenes);
+    wf_shadow<<<L.grid[3], L.block[3], trace_smem(L.block[3]), stream>>>(params, scenes);
     wf_advance<<<1, 1, 0, stream>>>(params, handle, use_handle);
     return cudaGetLastError();
 }

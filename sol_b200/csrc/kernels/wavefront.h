@@ -26,6 +26,14 @@ constexpr int kWfRefillBelow = SOL_WF_REFILL_BELOW;
 /// Resident 256-thread blocks per SM the traversal stages' registers must allow.
 constexpr int kWfTraceMinBlocks = SOL_WF_TRACE_MIN_BLOCKS;
 
+#ifndef SOL_WF_SHARED_STACK
+#define SOL_WF_SHARED_STACK 1
+#endif
+/// 1: the traversal stages keep the first kSharedStackDepth entries of each
+/// lane's stack in shared memory (dynamic, sized by the block), the rest in
+/// local memory; 0: the whole stack in local memory.
+constexpr bool kWfSharedStack = SOL_WF_SHARED_STACK != 0;
+
 /// Scenes one wavefront batch may hold: they travel with every stage launch as
 /// a kernel parameter, and a ray carries its scene's index in the bits above
 /// its slot number.
