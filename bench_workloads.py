@@ -131,6 +131,21 @@ def grad_check(g, fd, rel: float = GRAD_REL_TOL, floor_frac: float = 0.01) -> di
             "worst": None if worst < 0 else {"index": worst, "adjoint": float(g[worst]), "fd": float(fd[worst])}}
 
 
+def roulette_misses(g, fd, fd_half, check: dict) -> list:
+    """The parameters that miss the per-parameter tolerance, each with whether
+    its central difference jumps (changes by more than the tolerance when eps
+    halves): a Russian-roulette flip inside [x - eps, x + eps] makes the
+    estimator's difference quotient measure a jump, not the derivative."""
+    floor = check["abs_floor"]
+    out = []
+    for j, (a, f, h) in enumerate(zip(g, fd, fd_half)):
+        scale = max(abs(f), floor)
+        if abs(a - f) > check["tol_rel"] * scale:
+            out.append({"index": j, "adjoint": float(a), "fd": float(f), "fd_half_eps": float(h),
+                        "jumps": bool(abs(f - h) > check["tol_rel"] * scale)})
+    return out
+
+
 def fd_gradient(gs, render_loss, indices, eps: float = EPS):
     """Central differences of render_loss() over the given parameter indices."""
     base = gs.get_params()
@@ -459,6 +474,11 @@ def run_adjoint(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=Tru
     idx = choose_params(gs, 64, seed=5)
     fd = fd_gradient(gs, render_loss, idx)
     check = grad_check(g[idx], fd)
+    miss = [j for j in range(len(idx)) if abs(g[idx][j] - fd[j]) > GRAD_REL_TOL * max(abs(fd[j]), check["abs_floor"])]
+    if miss:   # central differences at eps / 2 for the misses (roulette jumps)
+        half = np.array(fd)
+        half[miss] = fd_gradient(gs, render_loss, [idx[j] for j in miss], eps=EPS / 2)
+        check["roulette_misses"] = roulette_misses(g[idx], fd, half, check)
     extra = {}
     if cpu:
         # SoL's renderer: its forward rate on the loss render, and central
@@ -604,7 +624,14 @@ def run_scenes(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=True
             return float(((f.double() / SPP - tgt) ** 2).sum())
         idx = choose_params(gs, 16, seed=100 + k)
         fd = fd_gradient(gs, render_loss, idx)
-        checks.append(grad_check(grads[k].cpu().numpy()[idx], fd))
+        gk = grads[k].cpu().numpy()[idx]
+        c = grad_check(gk, fd)
+        miss = [j for j in range(len(idx)) if abs(gk[j] - fd[j]) > GRAD_REL_TOL * max(abs(fd[j]), c["abs_floor"])]
+        if miss:   # central differences at eps / 2 for the misses (roulette jumps)
+            half = np.array(fd)
+            half[miss] = fd_gradient(gs, render_loss, [idx[j] for j in miss], eps=EPS / 2)
+            c["roulette_misses"] = [dict(m, scene=k) for m in roulette_misses(gk, fd, half, c)]
+        checks.append(c)
     extra = {}
     if cpu:
         # SoL's PathTracer on scenes 0 and 1 at their full size and 16 spp.
@@ -634,6 +661,7 @@ def run_scenes(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=True
                         "params_checked": int(sum(c["params"] for c in checks)),
                         "scenes_all_within_tol": int(sum(c["within_tol"] == c["params"] for c in checks)),
                         "max_rel_err_per_scene": [float(f"{c['max_rel_err']:.3g}") for c in checks],
+                        "roulette_misses": [m for c in checks for m in c.get("roulette_misses", [])],
                         "worst_scene": int(np.argmax([c["max_rel_err"] for c in checks])),
                         "worst": checks[int(np.argmax([c["max_rel_err"] for c in checks]))]["worst"]},
         e2e={"value": paths / mean["fused"] / 1e3, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -319,7 +319,7 @@ typedef struct SolGpuView {
 
 /* Tuning of the batch renderer; zero fields take defaults. */
 typedef struct SolGpuBatchOptions {
-    uint32_t capacity;        /* path slots in flight (default: 1M, at most the pixel count) */
+    uint32_t capacity;        /* path slots in flight (default: 4M, at most the work items) */
     uint32_t block_size;      /* threads per block of the stages: 64, 128 or 256 (default 128) */
     uint32_t sort_threshold;  /* bin hits by BSDF kind when at least this many rays are queued
                                  (0 = always; 0xffffffff = never) */

@@ -56,7 +56,7 @@ struct SolGpuBatch {
 
 namespace {
 
-constexpr uint32_t kDefaultCapacity = 1u << 20;
+constexpr uint32_t kDefaultCapacity = 1u << 22;
 constexpr uint32_t kMaxCapacity = 1u << 26;
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -410,6 +410,10 @@ int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVie
     if (e != cudaSuccess) return cuda_fail(e, "views upload");
     uint32_t want = b->opts.capacity ? b->opts.capacity : kDefaultCapacity;
     want = std::min<uint32_t>(std::max<uint32_t>(want, 32), kMaxCapacity);
+    // No more slots than the largest chunk has work items.
+    uint64_t most_items = 32;
+    for (const WfPass& pass : passes) most_items = std::max<uint64_t>(most_items, pass.total_items);
+    want = (uint32_t)std::min<uint64_t>(want, most_items);
     int rc = alloc_pool(b, want);
     if (rc != SOL_GPU_OK) return rc;
     rc = configure_launch(b);
@@ -712,7 +716,7 @@ int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const Sol
     size_t off = 0;
     for (auto& v : probe) { v.film = scratch + off; off += 3 * (size_t)v.width * v.height; v.sample_count = 1; }
     cudaStream_t s = b->capture;
-    const uint32_t caps[] = {1u << 18, 1u << 19, 1u << 20, 1u << 21, 1u << 22};
+    const uint32_t caps[] = {1u << 20, 1u << 21, 1u << 22, 1u << 23};
     const uint32_t blocks[] = {64, 128, 256};
     const uint32_t sorts[] = {0u, 1u << 16, 0xffffffffu};
     float best_ms = 1e30f;
