@@ -65,7 +65,7 @@ size_t pool_bytes(uint32_t c) {
     size_t b = 0;
     b += 9 * align256(sizeof(float4) * (size_t)c);                    // thru color ray_o[2] ray_d[2] sh_o sh_d sh_c
     b += align256(sizeof(unsigned long long) * (size_t)c);            // rng
-    b += align256(sizeof(uint4) * (size_t)c);                         // pix
+    b += align256(sizeof(uint2) * (size_t)c);                         // item
     b += align256(sizeof(float2) * (size_t)c);                        // hit
     b += (2 + kWfBins) * align256(sizeof(uint32_t) * (size_t)c);      // ended queues, bins
     return b;
@@ -94,7 +94,7 @@ int alloc_pool(SolGpuBatch* b, uint32_t capacity) {
     h.thru = reinterpret_cast<float4*>(take(sizeof(float4) * c));
     h.color = reinterpret_cast<float4*>(take(sizeof(float4) * c));
     h.rng = reinterpret_cast<unsigned long long*>(take(sizeof(unsigned long long) * c));
-    h.pix = reinterpret_cast<uint4*>(take(sizeof(uint4) * c));
+    h.item = reinterpret_cast<uint2*>(take(sizeof(uint2) * c));
     for (int k = 0; k < 2; ++k) {
         h.ray_o[k] = reinterpret_cast<float4*>(take(sizeof(float4) * c));
         h.ray_d[k] = reinterpret_cast<float4*>(take(sizeof(float4) * c));
@@ -288,12 +288,17 @@ int render_megakernel(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVi
     }
 }
 
+/// Work items of one sample of a view: its 8x4 pixel tiles, 32 items each.
+uint64_t items_per_sample(const SolGpuView& v) {
+    return (uint64_t)((v.width + 7) / 8) * ((v.height + 3) / 4) * 32;
+}
+
 /// One launch of the wavefront over a set of views (one chunk of samples).
 struct WfPass {
     size_t first_view = 0;   // into the concatenated view tables
     uint32_t num_views = 0;
     uint32_t total_items = 0;
-    uint64_t sum_floats = 0;
+    uint64_t sum_pixels = 0;   // pixels of the pass's views (threads of its sum pass)
 };
 
 /// The wavefront: views are split into (sample, pixel) work items whose path
@@ -314,15 +319,17 @@ int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVie
         if (s.width == 0 || s.height == 0) return fail(SOL_GPU_ERR_INVALID_ARG, "view size must be positive");
         if (!s.film) return fail(SOL_GPU_ERR_INVALID_ARG, "view film must not be NULL");
         max_spp = std::max(max_spp, s.sample_count);
-        all_floats += 3ull * s.width * s.height * s.sample_count;
+        all_floats += 4ull * items_per_sample(s) * s.sample_count;
     }
     const uint64_t limit = (b->scratch_limit ? b->scratch_limit : kWfScratchMaxBytes) / sizeof(float);
-    auto need = [&](uint32_t k) {   // scratch floats of chunks of k samples: first chunk + running sums
+    // Scratch floats of chunks of k samples: one float4 per work item of the
+    // first chunk (item order), plus 3 planes of running sums per view that
+    // needs more than one chunk.
+    auto need = [&](uint32_t k) {
         uint64_t f = 0;
         for (uint32_t i = 0; i < n; ++i) {
-            const uint64_t plane = 3ull * views[i].width * views[i].height;
-            f += plane * std::min(k, views[i].sample_count);
-            if (views[i].sample_count > k) f += plane;
+            f += 4ull * items_per_sample(views[i]) * std::min(k, views[i].sample_count);
+            if (views[i].sample_count > k) f += 3ull * views[i].width * views[i].height;
         }
         return f;
     };
@@ -347,7 +354,7 @@ int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVie
     std::vector<uint64_t> running_at(n, 0);
     {
         uint64_t at = 0;
-        for (uint32_t i = 0; i < n; ++i) at += 3ull * views[i].width * views[i].height * std::min(chunk, views[i].sample_count);
+        for (uint32_t i = 0; i < n; ++i) at += 4ull * items_per_sample(views[i]) * std::min(chunk, views[i].sample_count);
         for (uint32_t i = 0; i < n; ++i)
             if (views[i].sample_count > chunk) { running_at[i] = at; at += 3ull * views[i].width * views[i].height; }
     }
@@ -377,13 +384,12 @@ int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVie
             w.item_begin = (uint32_t)items;
             w.split = 1;
             w.scratch = b->scratch + scratch_at;
-            w.sum_begin = pass.sum_floats;
+            w.sum_begin = pass.sum_pixels;
             w.running = s.sample_count > chunk ? b->scratch + running_at[i] : nullptr;
             w.first_chunk = c0 == 0;
             w.last_chunk = c0 + k >= s.sample_count;
-            const uint64_t plane3 = 3ull * s.width * s.height;
-            scratch_at += plane3 * k;
-            pass.sum_floats += plane3;
+            scratch_at += 4ull * items_per_sample(s) * k;
+            pass.sum_pixels += (uint64_t)s.width * s.height;
             items += (uint64_t)w.tiles_x * ((s.height + 3) / 4) * 32 * k;
             paths += (uint64_t)s.width * s.height * k;
             if (items > 0xffffffffull) return fail(SOL_GPU_ERR_INVALID_ARG, "batch too large (more than 2^32 work items)");
@@ -424,8 +430,11 @@ int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVie
     h.cfg = to_config(*config);
     h.ctr = b->d_ctr;
     cudaEventRecord(b->ev_start, stream);
+    bool first_pass = true;
     for (const WfPass& pass : passes) {
         if (pass.num_views == 0) continue;
+        h.keep_counts = first_pass ? 0u : 1u;   // counters add up over the chunks of samples
+        first_pass = false;
         h.capacity = (uint32_t)std::min<uint64_t>(want, std::max<uint64_t>(pass.total_items, 32));
         h.num_views = pass.num_views;
         h.total_items = pass.total_items;
@@ -455,7 +464,7 @@ int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVie
                 if (it > h.max_iterations) return fail(SOL_GPU_ERR_TIMEOUT, "bounce loop exceeded its bound");
             }
         }
-        e = launch_sum_samples_views(h.views, pass.num_views, pass.sum_floats, stream);
+        e = launch_sum_items_views(h.views, pass.num_views, pass.sum_pixels, stream);
         if (e != cudaSuccess) return cuda_fail(e, "sum pass");
     }
     cudaEventRecord(b->ev_stop, stream);

@@ -106,6 +106,11 @@ cudaError_t launch_megakernel_views(const WfView* views, uint32_t num_views, uin
 cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, uint64_t total_floats,
                                      cudaStream_t stream);
 
+/// Sum pass of the wavefront's views (item-ordered float4 scratch, see
+/// WfView): one thread per pixel of the views laid end to end from
+/// WfView::sum_begin (`total_pixels` in all).
+cudaError_t launch_sum_items_views(const WfView* views, uint32_t num_views, uint64_t total_pixels, cudaStream_t stream);
+
 /// K9: closest-hit or any-hit queries for a batch of rays.
 cudaError_t launch_trace(const SceneView& s, const SolGpuRay* rays, uint32_t count, bool any_hit,
                          SolGpuHit* hits, cudaStream_t stream);

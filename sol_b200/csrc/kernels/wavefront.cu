@@ -32,6 +32,8 @@
 // are bit-identical to the megakernel's.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "kernels.h"
 #include "path.cuh"
 #include "wavefront.h"
@@ -95,7 +97,7 @@ __global__ void __launch_bounds__(256) wf_init(const WfParams* __restrict__ Pp) 
     const WfParams& P = *Pp;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.capacity; i += gridDim.x * blockDim.x) {
         P.q_ended[0][i] = i;
-        P.pix[i] = make_uint4(kIdle, 0, 0, 0);
+        P.item[i] = make_uint2(kIdle, 0);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         WfCounters* c = P.ctr;
@@ -108,12 +110,12 @@ __global__ void __launch_bounds__(256) wf_init(const WfParams* __restrict__ Pp) 
         c->next_item = 0;
         c->iter = 0;
         c->more = 1;
-        c->paths = c->rays = c->shadow_rays = 0;
+        if (!P.keep_counts) c->paths = c->rays = c->shadow_rays = 0;
         c->error = 0;
     }
 }
 
-/// K2: ended paths write their colour to the scratch of their (view, sample);
+/// K2: ended paths write their colour to the scratch of their work item;
 /// their slots claim the next work items and start the camera rays.
 __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ Pp) {
     const WfParams& P = *Pp;
@@ -126,19 +128,14 @@ __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ 
         const uint32_t i = base + threadIdx.x;
         if (i >= n) continue;
         const uint32_t slot = P.q_ended[p][i];
-        uint4 px = P.pix[slot];
+        uint2 it = P.item[slot];
         float4 col = P.color[slot];
         uint32_t claims = 0;
         while (true) {
-            if (px.x != kIdle) {
+            if (it.x != kIdle) {
                 // path_tracer.cpp:19 -- the pixel's sum is formed by the sum pass
-                const WfView& v = P.views[px.x];
-                const size_t plane = (size_t)v.width * v.height;
-                float* f = v.scratch + (size_t)px.w * 3u * plane + (size_t)px.z * v.width + px.y;
-                f[0] = col.x;
-                f[plane] = col.y;
-                f[2 * plane] = col.z;
-                px.x = kIdle;
+                reinterpret_cast<float4*>(P.views[it.x].scratch)[it.y] = make_float4(col.x, col.y, col.z, 0.0f);
+                it.x = kIdle;
             }
             if (++claims > total + 2u) { atomicOr(&ctr->error, kFaultClaimLoop); break; }
             const uint32_t item = append(&ctr->next_item);
@@ -146,17 +143,17 @@ __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ 
             const uint32_t vi = find_view(P.views, P.num_views, item);
             const WfView& v = P.views[vi];
             const uint32_t per_sample = v.tiles_x * ((v.height + 3u) / 4u) * 32u;
-            uint32_t local = item - v.item_begin;
+            const uint32_t local = item - v.item_begin;
             const uint32_t k = local / per_sample;
-            local -= k * per_sample;
-            const uint32_t tile = local >> 5, l = local & 31u;
+            const uint32_t in_sample = local - k * per_sample;
+            const uint32_t tile = in_sample >> 5, l = in_sample & 31u;
             const uint32_t x = (tile % v.tiles_x) * 8u + (l & 7u);
             const uint32_t y = (tile / v.tiles_x) * 4u + (l >> 3);
-            if (x >= v.width || y >= v.height) continue;
+            if (x >= v.width || y >= v.height) continue;   // padding of a partial tile: no pixel
             PathState ps;
             start_path(ps, view_camera(v), v.sample_index + k, x, y, v.width, v.height);
             ++paths;
-            px = make_uint4(vi, x, y, k);
+            it = make_uint2(vi, local);
             col = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             if (P.cfg.max_path_len == 0) continue;   // empty path: black, written above
             P.thru[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -167,17 +164,49 @@ __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ 
             P.ray_d[p][q] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, tag_bits(slot, v.scene));
             break;
         }
-        P.pix[slot] = px;
+        P.item[slot] = it;
     }
     paths = warp_sum(paths);
     if (lane_id() == 0 && paths) atomicAdd(&ctr->paths, paths);
 }
 
-/// Persistent traversal of a ray queue with dynamic ray fetch: every lane keeps
-/// one ray; at the top of each round the warp claims queue entries for its idle
-/// lanes with one atomic, then traverses until the ray is done or the warp has
-/// fewer than `refill_below` busy lanes.  `fetch(i, tr, stack) -> scene`
-/// starts queue entry i; `finish(i, tr)` consumes a finished ray.
+/// The wavefront's sum pass: one thread per pixel of the views laid end to end
+/// from WfView::sum_begin adds the pixel's path colours (item-ordered float4
+/// scratch) in sample order to its running sum -- 0 for a view's first chunk
+/// of samples -- and the last chunk adds the sum into the film, so each
+/// channel sees the additions of SoL's per-pixel loop (path_tracer.cpp:15-21).
+__global__ void __launch_bounds__(256)
+sum_items_views(const WfView* __restrict__ views, uint32_t num_views, uint64_t total) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total; g += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = num_views;
+        while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (views[mid].sum_begin <= g) lo = mid; else hi = mid; }
+        const WfView& V = views[lo];
+        const uint32_t px = (uint32_t)(g - V.sum_begin);
+        const uint32_t x = px % V.width, y = px / V.width;
+        const size_t plane = (size_t)V.width * V.height;
+        const uint32_t per_sample = V.tiles_x * ((V.height + 3u) / 4u) * 32u;
+        const uint32_t at = ((y >> 2) * V.tiles_x + (x >> 3)) * 32u + (y & 3u) * 8u + (x & 7u);
+        const float4* __restrict__ c = reinterpret_cast<const float4*>(V.scratch) + at;
+        float r = 0.0f, gg = 0.0f, b = 0.0f;
+        if (!V.first_chunk) { r = V.running[px]; gg = V.running[px + plane]; b = V.running[px + 2 * plane]; }
+        for (uint32_t k = 0; k < V.sample_count; ++k) {
+            const float4 v = c[(size_t)k * per_sample];
+            r += v.x;
+            gg += v.y;
+            b += v.z;
+        }
+        if (V.last_chunk) {
+            V.film[px] += r;
+            V.film[px + plane] += gg;
+            V.film[px + 2 * plane] += b;
+        } else {
+            V.running[px] = r;
+            V.running[px + plane] = gg;
+            V.running[px + 2 * plane] = b;
+        }
+    }
+}
+
 /// The traversal stack of a trace-stage lane (see kWfSharedStack).
 #if SOL_WF_SHARED_STACK
 using WfStack = SharedStackDyn;
@@ -405,6 +434,13 @@ int wavefront_blocks_per_sm(int stage, int block) {
         default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow, block, trace_smem(block)); break;
     }
     return e == cudaSuccess ? n : -1;
+}
+
+cudaError_t launch_sum_items_views(const WfView* views, uint32_t num_views, uint64_t total_pixels, cudaStream_t stream) {
+    if (total_pixels == 0) return cudaSuccess;
+    const int blocks = (int)std::min<uint64_t>((total_pixels + 255) / 256, 8192);
+    sum_items_views<<<blocks, 256, 0, stream>>>(views, num_views, total_pixels);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_wf_init(const WfParams* params, uint32_t capacity, cudaStream_t stream) {

@@ -52,8 +52,11 @@ struct WfSceneTable {
 /// Work items are 8x4 pixel tiles of 32 items each; split views (every
 /// wavefront view, and the multi-view megakernel's views of more than one
 /// sample) have one item per (sample, pixel), taken sample-major, and write
-/// each path's colour to `scratch` (sample_count x 3 planes); the sum pass then
-/// adds every pixel's colours in sample order.
+/// each path's colour to `scratch`, which the sum pass adds per pixel in sample
+/// order.  The multi-view megakernel's scratch is sample_count x 3 planes of
+/// the image; the wavefront's is one float4 per work item, in item order (the
+/// items in flight are a contiguous range, so their colours land in a few MB
+/// that L2 keeps until every 32-byte sector is complete).
 struct WfView {
     float eye[3], dir[3], right[3], up[3];
     uint32_t scene;          // index into the batch's scenes
@@ -100,6 +103,7 @@ struct WfParams {
     uint32_t total_items;
     unsigned long long max_iterations;   // self-check bound on bounce-loop iterations
     int refill_below;        // a traversal warp refills its idle lanes when fewer than this many are busy
+    uint32_t keep_counts;    // 1: add this launch's paths and rays to the counters instead of restarting them
     DConfig cfg;
     const WfView* views;
     WfCounters* ctr;
@@ -107,7 +111,7 @@ struct WfParams {
     float4* thru;            // throughput, pdf_prev
     float4* color;           // radiance gathered so far, path_len (bits)
     unsigned long long* rng;
-    uint4* pix;              // view, x, y, sample number within the launch (view = idle: none)
+    uint2* item;             // the slot's work item: view, item within the view (view = idle: none)
     // per queue position
     float4* ray_o[2];        // extend queue by parity: origin, tmin
     float4* ray_d[2];        //                         direction, slot | scene << kWfSlotBits (bits)
