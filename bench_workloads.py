@@ -132,10 +132,11 @@ def grad_check(g, fd, rel: float = GRAD_REL_TOL, floor_frac: float = 0.01) -> di
 
 
 def roulette_misses(g, fd, fd_half, check: dict) -> list:
-    """The parameters that miss the per-parameter tolerance, each with whether
-    its central difference jumps (changes by more than the tolerance when eps
-    halves): a Russian-roulette flip inside [x - eps, x + eps] makes the
-    estimator's difference quotient measure a jump, not the derivative."""
+    """The parameters that miss the per-parameter tolerance, with their central
+    differences at eps and eps / 2.  With Russian roulette on, a survival
+    decision that flips inside [x - eps, x + eps] adds its jump to the
+    difference quotient (and, the loss being quadratic, the jump's square
+    always with the same sign), which no derivative of the estimate has."""
     floor = check["abs_floor"]
     out = []
     for j, (a, f, h) in enumerate(zip(g, fd, fd_half)):
@@ -146,19 +147,28 @@ def roulette_misses(g, fd, fd_half, check: dict) -> list:
     return out
 
 
+def fd_step(value: float, eps: float = EPS) -> float:
+    """The central-difference step of a parameter: eps, scaled by the value
+    above 1 (emissions of 10-20 move the float32 film by less than its
+    rounding at an absolute step of 1e-3)."""
+    return eps * max(1.0, abs(float(value)))
+
+
 def fd_gradient(gs, render_loss, indices, eps: float = EPS):
-    """Central differences of render_loss() over the given parameter indices."""
+    """Central differences of render_loss() over the given parameter indices
+    (step fd_step(value, eps) per parameter)."""
     base = gs.get_params()
     out = []
     for j in indices:
+        h = fd_step(base[j], eps)
         v = base.copy()
-        v[j] = base[j] + eps
+        v[j] = base[j] + h
         gs.set_params(v)
         lp = render_loss()
-        v[j] = base[j] - eps
+        v[j] = base[j] - h
         gs.set_params(v)
         lm = render_loss()
-        out.append((lp - lm) / (2.0 * eps))
+        out.append((lp - lm) / (2.0 * h))
     gs.set_params(base)
     return np.asarray(out)
 

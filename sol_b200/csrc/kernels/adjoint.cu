@@ -7,14 +7,13 @@
 // replayed from its seed (Path Replay Backpropagation; Vicini, Speierer, Jakob,
 // SIGGRAPH 2021), so no path is stored between kernels.  Geometry is fixed, so
 // colour values change no sampled direction and no visibility; their derivative
-// along each replayed path is exact, with the Russian roulette survival
-// probability q = clamp(lum(T)) (path_tracer.cpp:100-107) held constant.  A
-// surviving path carries 1/q; the derivative of 1/q along the path is
-// cancelled, in expectation, by the change of the probability that the path
-// survives at all (the draw crossing q), which no replay sees -- so the
-// estimator that leaves q out is the unbiased one for the derivative of the
-// expected image, and it is what a central difference with common random
-// numbers measures once its interval holds many survival flips.
+// along each replayed path is exact, including the dependence of the Russian
+// roulette probability clamp(lum(T)) on the throughput (path_tracer.cpp:100-107):
+// it is the derivative of the estimate the forward computes, which central
+// differences with common random numbers converge to.  (Holding the
+// probability constant instead, as for an estimator of the expected image's
+// derivative, was measured off by up to 4x from those differences on the
+// Cornell box at path length 16, where throughputs pass many roulette tests.)
 // A Phong exponent also shapes the lobe the bounce is sampled from; its
 // derivative is taken with sampling detached (the sampled directions, their
 // pdfs and the MIS weights held fixed, as in PRB): per vertex the BSDF value's
@@ -47,7 +46,7 @@ namespace sol_b200 {
 
 namespace {
 
-constexpr uint32_t kEmit = 1u, kNee = 2u, kBounce = 4u;
+constexpr uint32_t kEmit = 1u, kNee = 2u, kBounce = 4u, kRrLive = 8u;
 
 /// A texture value's factor in a colour: colour = value * scale (per channel).
 struct TexTerm {
@@ -72,6 +71,7 @@ struct VertexRec {
     TexTerm cterm[2];
     ScalarTerm nterm[2];        // d f / d (Phong exponent) of the light sample's BSDF value
     ScalarTerm bterm[2];        // d c / d (Phong exponent) of the bounce
+    float q;                    // Russian roulette survival probability
     Vec2 uv;                    // shading texture coordinates
     uint32_t flags;
 };
@@ -330,6 +330,7 @@ struct Recorder {
         R->flags = 0;
         R->T = ps.T;
         R->uv = sf.uv;
+        R->q = 1.0f;
         R->fterm[0] = R->fterm[1] = R->cterm[0] = R->cterm[1] = TexTerm{-1, 0.0f};
         R->nterm[0] = R->nterm[1] = R->bterm[0] = R->bterm[1] = ScalarTerm{-1, rgb(0.0f)};
     }
@@ -359,8 +360,10 @@ struct Recorder {
         eval_terms(s, bsdf_id, in_dir, sf, out_dir, R->fterm);
         exponent_terms(s, bsdf_id, in_dir, sf, out_dir, R->nterm);
     }
-    // The survival probability is held constant by the sweep: nothing to keep.
-    __device__ __forceinline__ void survival(float, bool) {}
+    __device__ __forceinline__ void survival(float q, bool live) {
+        R->q = q;
+        if (live) R->flags |= kRrLive;
+    }
     __device__ __forceinline__ void before_bounce(const SceneView& s, int bsdf_id, const Surface& sf, const Pcg& rng) {
         // Which operand an InterpBsdf samples is its first draw (bsdfs.cpp:192-198).
         const DBsdf b = s.bsdfs[bsdf_id];
@@ -488,8 +491,13 @@ __device__ SOL_ADJ_OUTLINE void sweep(const SceneView& s, const VertexRec* rec, 
             const Rgb w = a * R.T * R.r;
             terms.colors(R.cterm, w);
             terms.scalars(R.bterm, w);
-            // r = cos / (pdf q): q, the survival probability, is held constant (see above).
             aT = a * R.c * R.r;
+            if (R.flags & kRrLive) {
+                // r = cos / (pdf q) with q = clamp(lum(T)): d r / d T = -r / q * d lum / d T.
+                const Rgb aTc = a * R.T * R.c;
+                const float a_q = -(aTc.r + aTc.g + aTc.b) * R.r / R.q;
+                aT = aT + rgb(0.2126f * a_q, 0.7152f * a_q, 0.0722f * a_q);
+            }
         }
         if (R.flags & kNee) {
             aT = aT + G * R.Ls * R.f * R.s;

@@ -117,9 +117,10 @@ def test_scene_set_fused_forward_adjoint_matches_sol(built):
 def test_converged_cornell_matches_sol(built):
     """1024 samples per pixel of the 64x64 Cornell box: the GPU film and SoL's
     at the same sample indices agree to RMSE <= 1e-6 of the mean (the same
-    estimator).  For scale, the Monte Carlo error: the RMSE between two
-    disjoint sample ranges falls as 1/sqrt(samples) -- from 1024 to 4096
-    samples it must shrink by a factor between 1.6 and 2.5 (2 expected)."""
+    estimator).  For scale, the Monte Carlo error between two disjoint sample
+    ranges: its per-pixel median falls as 1/sqrt(samples), by a factor between
+    1.6 and 2.5 (2 expected) from 1024 to 4096 samples.  (The RMSE falls more
+    slowly: the glass box's caustic paths are rare and bright, a heavy tail.)"""
     from sol_b200 import scenes
     from sol_b200.renderer import GpuPathTracer, Image
     scene, cfg, *_ = scenes.cornell_frame()
@@ -134,9 +135,11 @@ def test_converged_cornell_matches_sol(built):
     a = film(0, N)
     mean = float(cpu.mean() / N)
     rmse_same = float(np.sqrt(np.mean((a - cpu / N) ** 2)))
-    r1 = float(np.sqrt(np.mean((a - film(N, N)) ** 2)))
-    r4 = float(np.sqrt(np.mean((film(1 << 16, 4 * N) - film(1 << 17, 4 * N)) ** 2)))
-    print(f"converged 64x64: mean {mean:.4f}, RMSE vs SoL at the same samples {rmse_same:.3g}; "
-          f"disjoint ranges: {r1:.4f} at {N} spp, {r4:.4f} at {4 * N} spp")
+    d1 = np.abs(a - film(N, N))
+    d4 = np.abs(film(1 << 16, 4 * N) - film(1 << 17, 4 * N))
+    m1, m4 = float(np.median(d1)), float(np.median(d4))
+    print(f"converged 64x64: mean {mean:.4f}, RMSE vs SoL at the same samples {rmse_same:.3g}; disjoint ranges: "
+          f"median |diff| {m1:.5f} at {N} spp, {m4:.5f} at {4 * N} spp; RMSE {np.sqrt(np.mean(d1 ** 2)):.4f}, "
+          f"{np.sqrt(np.mean(d4 ** 2)):.4f}")
     assert rmse_same <= 1e-6 * mean
-    assert 1.6 <= r1 / r4 <= 2.5
+    assert 1.6 <= m1 / m4 <= 2.5
