@@ -47,12 +47,13 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--small", action="store_true", help="quick run on a reduced frame (not a bench number)")
-    p.add_argument("--workload", default="frame", choices=["frame", "cornell", "views", "adjoint", "scenes"],
+    p.add_argument("--workload", default="frame", choices=["frame", "cornell", "views", "adjoint", "scenes", "stages"],
                    help="frame: one large frame per render call (default; the other configurations are added "
                         "under `configs`); cornell: the Cornell box at 256^2 x 16 spp; views: 64 uneven views of a "
                         "4,194,314-triangle field, batched vs 64 plain launches; adjoint: path-replay adjoint vs "
                         "forward on the textured Cornell box; scenes: fused forward + adjoint over 32 independent "
-                        "scenes")
+                        "scenes; stages: one wavefront render of the views workload through the host-driven loop, "
+                        "for profiler launch lists")
     p.add_argument("--no-configs", action="store_true", help="frame only: skip the other configurations")
     return p.parse_args()
 

@@ -678,7 +678,37 @@ def run_scenes(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=True
         scene_generation_s=gen_s, bvh_build_ms=float(sum(i.build_ms for i in infos)), **extra)
 
 
-RUNS = {"cornell": run_cornell, "views": run_views, "adjoint": run_adjoint, "scenes": run_scenes}
+def run_stages(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=False):
+    """One wavefront render of the views workload (or, with --small, 16 views
+    of at most 512^2 at 8 spp of the 1M-triangle field) through the
+    host-driven bounce loop, which launches the same stage kernels as the
+    CUDA graph one by one, so that a profiler lists them (kernels inside a
+    graph's WHILE body are not profiled)."""
+    import torch
+    from sol_b200 import capi, scenes
+    from sol_b200.renderer import BatchRenderer, GpuScene
+    cfg = scenes.SPHERES_CONFIG
+    if args.small:
+        scene = scenes.sphere_field(64, seed=1)
+        views = [(c, s, 8) for c, s, _ in scenes.view_set(16, seed=2, max_side=512)]
+    else:
+        scene = scenes.sphere_field(256, seed=1)
+        views = scenes.view_set(64, seed=2)
+    gs = GpuScene(scene)
+    films = [torch.zeros((3, s, s), device="cuda") for _, s, _ in views]
+    br = BatchRenderer([gs], capacity=1 << 22, block_size=256, sort_threshold=0, host_loop=True,
+                       schedule=capi.BATCH_WAVEFRONT)
+    arr = br.views([(0, c, s, s, 0, p, f.data_ptr()) for (c, s, p), f in zip(views, films)])
+    br.render(cfg, arr)
+    torch.cuda.synchronize()
+    st = br.stats()
+    return {"metric": "wavefront render through the host-driven loop", "value": st.kernel_ms, "unit": "ms",
+            "paths": st.paths, "rays": st.rays, "shadow_rays": st.shadow_rays, "views": len(views),
+            "small": bool(args.small), "note": "for profiler launch lists; not a bench number"}
+
+
+RUNS = {"cornell": run_cornell, "views": run_views, "adjoint": run_adjoint, "scenes": run_scenes,
+        "stages": run_stages}
 
 
 def run(args, ClockSampler, load_peaks) -> int:
