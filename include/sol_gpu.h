@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define SOL_GPU_ABI_VERSION 2
+#define SOL_GPU_ABI_VERSION 3
 
 /* Status codes */
 #define SOL_GPU_OK                  0
@@ -325,7 +325,17 @@ typedef struct SolGpuBatchOptions {
                                  (0 = always; 0xffffffff = never) */
     int32_t host_loop;        /* 1: bounce loop driven from the host instead of the graph */
     int32_t schedule;         /* SOL_GPU_BATCH_WAVEFRONT, _MEGAKERNEL or _AUTO (below) */
+    int32_t ray_order;        /* SOL_GPU_RAY_ORDER_* (below); ABI version 3 */
 } SolGpuBatchOptions;
+
+/* Order in which the wavefront traces each bounce's rays.  QUEUE: as the
+ * stages queued them.  SORTED: counting-sorted first by scene, direction
+ * octant and the Morton cell of the origin, so that neighbouring lanes walk
+ * the same part of the hierarchy.  DEFAULT (0) is SORTED.  Films are the same
+ * bits either way. */
+#define SOL_GPU_RAY_ORDER_DEFAULT 0
+#define SOL_GPU_RAY_ORDER_QUEUE   1
+#define SOL_GPU_RAY_ORDER_SORTED  2
 
 /* Batch schedules.  WAVEFRONT: the queue-based wavefront (capacity, block size
  * and sort threshold apply).  MEGAKERNEL: one persistent megakernel launch over
@@ -368,7 +378,7 @@ int sol_gpu_batch_set_scratch_limit(SolGpuBatch* batch, uint64_t bytes);
  * timeout, src/render_job.cpp:42-55, bounds a host wait, not the loop). */
 int sol_gpu_batch_set_iteration_limit(SolGpuBatch* batch, uint64_t max_iterations);
 
-/* Times candidate options (capacity, block size, binning threshold; with
+/* Times candidate options (capacity, block size, binning threshold, ray order; with
  * schedule AUTO also the megakernel schedule) on one sample per pixel of the
  * given views, rendered into scratch films, adopts the fastest and returns it
  * in `chosen`.  With `cache_path` set, a previous

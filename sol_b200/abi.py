@@ -21,6 +21,7 @@ ERR_UNSUPPORTED = -7
 ERR_CANCELLED = -8
 SCHEDULE_AUTO, SCHEDULE_PER_PIXEL, SCHEDULE_SPLIT = 0, 1, 2
 BATCH_WAVEFRONT, BATCH_MEGAKERNEL, BATCH_AUTO = 0, 1, 2
+RAY_ORDER_DEFAULT, RAY_ORDER_QUEUE, RAY_ORDER_SORTED = 0, 1, 2
 SCENE_GPU_BVH = 1
 
 BSDF_DIFFUSE, BSDF_PHONG, BSDF_MIRROR, BSDF_GLASS, BSDF_INTERP = range(5)
@@ -107,7 +108,7 @@ class SolGpuAdjointView(C.Structure):
 
 class SolGpuBatchOptions(C.Structure):
     _fields_ = [("capacity", C.c_uint32), ("block_size", C.c_uint32), ("sort_threshold", C.c_uint32),
-                ("host_loop", C.c_int32), ("schedule", C.c_int32)]
+                ("host_loop", C.c_int32), ("schedule", C.c_int32), ("ray_order", C.c_int32)]
 
 
 ScenePtr = C.c_void_p

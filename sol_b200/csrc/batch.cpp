@@ -39,6 +39,9 @@ struct SolGpuBatch {
     float* scratch = nullptr;         // per-sample colours of split views (and the wavefront's running sums)
     uint64_t scratch_floats = 0;
     WfSceneTable wf_table{};          // the scenes as the wavefront stages take them (kernel parameter)
+    float4* d_scene_box = nullptr;    // per scene: bounds of the hierarchy's root (reordering keys)
+    uint32_t* d_sort_bins = nullptr;  // reordering histogram and offsets
+    bool graph_sort = false;          // the captured graph reorders the queues
     bool basic = false;               // every scene has basic shading
     unsigned long long max_iterations = 0;   // wavefront bounce-loop bound (0: the default)
     uint64_t scratch_limit = 0;       // wavefront scratch bytes per render (0: kWfScratchMaxBytes)
@@ -68,6 +71,8 @@ size_t pool_bytes(uint32_t c) {
     b += align256(sizeof(uint2) * (size_t)c);                         // item
     b += align256(sizeof(float2) * (size_t)c);                        // hit
     b += (2 + kWfBins) * align256(sizeof(uint32_t) * (size_t)c);      // ended queues, bins
+    b += 3 * align256(sizeof(float4) * (size_t)c);                    // reordering: spare arrays
+    b += align256(sizeof(uint32_t) * (size_t)c);                      // reordering: keys
     return b;
 }
 
@@ -104,6 +109,8 @@ int alloc_pool(SolGpuBatch* b, uint32_t capacity) {
     h.sh_o = reinterpret_cast<float4*>(take(sizeof(float4) * c));
     h.sh_d = reinterpret_cast<float4*>(take(sizeof(float4) * c));
     h.sh_c = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    for (int k = 0; k < 3; ++k) h.alt[k] = reinterpret_cast<float4*>(take(sizeof(float4) * c));
+    h.sort_key = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
     h.q_bins = reinterpret_cast<uint32_t*>(p);
     return SOL_GPU_OK;
 }
@@ -118,6 +125,7 @@ int configure_launch(SolGpuBatch* b) {
         b->launch.grid[s] = per_sm * b->num_sms;
         b->launch.block[s] = block;
     }
+    b->launch.sms = b->num_sms;
     b->launch_block = block;
     destroy_graph(b);
     return SOL_GPU_OK;
@@ -140,7 +148,8 @@ int build_graph(SolGpuBatch* b) {
     cudaGraph_t body = np.conditional.phGraph_out[0];
     e = cudaStreamBeginCaptureToGraph(b->capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        cudaError_t le = launch_wf_iteration(b->d_params, b->wf_table, b->basic, b->launch, handle, 1, b->capture);
+        cudaError_t le = launch_wf_iteration(b->d_params, b->wf_table, b->basic, b->graph_sort, b->launch, handle, 1,
+                                             b->capture);
         e = cudaStreamEndCapture(b->capture, &body);
         if (e == cudaSuccess) e = le;
     }
@@ -425,6 +434,19 @@ int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVie
     rc = configure_launch(b);
     if (rc != SOL_GPU_OK) return rc;
     WfParams& h = b->host;
+    const bool ray_sort = b->opts.ray_order != SOL_GPU_RAY_ORDER_QUEUE;
+    if (ray_sort != b->graph_sort) {
+        destroy_graph(b);
+        b->graph_sort = ray_sort;
+    }
+    h.ray_sort = ray_sort ? 1u : 0u;
+    {
+        uint32_t bits = 0;
+        while ((1u << bits) < b->scenes.size()) ++bits;
+        h.scene_bits = bits;
+    }
+    h.scene_box = b->d_scene_box;
+    h.sort_bins = b->d_sort_bins;
     h.sort_threshold = b->opts.sort_threshold;
     h.refill_below = kWfRefillBelow;
     h.cfg = to_config(*config);
@@ -456,7 +478,7 @@ int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVie
             // Host-driven loop: the same stages, one iteration per round trip.
             cudaGraphConditionalHandle none{};
             for (uint64_t it = 0;; ++it) {
-                e = launch_wf_iteration(b->d_params, b->wf_table, b->basic, b->launch, none, 0, stream);
+                e = launch_wf_iteration(b->d_params, b->wf_table, b->basic, ray_sort, b->launch, none, 0, stream);
                 if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_ctr, b->d_ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
                 if (e != cudaSuccess) return cuda_fail(e, "wavefront iteration");
@@ -508,6 +530,7 @@ bool read_cache(const char* path, const std::string& key, SolGpuBatchOptions* o)
         SolGpuBatchOptions r{};
         if (std::getline(in, k, '\t') && (in >> r.capacity >> r.block_size >> r.sort_threshold) && k == key) {
             if (!(in >> r.schedule)) r.schedule = SOL_GPU_BATCH_WAVEFRONT;
+            if (!(in >> r.ray_order)) r.ray_order = SOL_GPU_RAY_ORDER_DEFAULT;
             *o = r;
             found = true;
         }
@@ -544,6 +567,26 @@ int sol_gpu_batch_create(SolGpuScene* const* scenes, uint32_t num_scenes, const 
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_ctr), sizeof(WfCounters));
     if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_scenes), sizeof(SceneView) * num_scenes);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_scenes, views.data(), sizeof(SceneView) * num_scenes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        // Scene bounds for the reordering keys: the union of the root's two child boxes.
+        std::vector<float4> boxes(2 * (size_t)num_scenes, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+        for (uint32_t i = 0; i < num_scenes && e == cudaSuccess; ++i) {
+            boxes[2 * i + 1] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            if (scenes[i]->view.num_nodes == 0) continue;
+            DNode root{};
+            e = cudaMemcpy(&root, scenes[i]->nodes, sizeof(DNode), cudaMemcpyDeviceToHost);
+            boxes[2 * i] = make_float4(std::min(root.b0[0], root.b1[0]), std::min(root.b0[2], root.b1[2]),
+                                       std::min(root.b2[0], root.b2[2]), 0.0f);
+            boxes[2 * i + 1] = make_float4(std::max(root.b0[1], root.b1[1]), std::max(root.b0[3], root.b1[3]),
+                                           std::max(root.b2[1], root.b2[3]), 0.0f);
+        }
+        if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_scene_box), sizeof(float4) * boxes.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b->d_scene_box, boxes.data(), sizeof(float4) * boxes.size(), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_sort_bins), 2 * sizeof(uint32_t) * kWfSortBins);
+    if (e == cudaSuccess) e = cudaMemset(b->d_sort_bins, 0, 2 * sizeof(uint32_t) * kWfSortBins);
+    if (e == cudaSuccess) e = allow_sort_smem();
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&b->h_ctr), sizeof(WfCounters));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&b->ev_start);
@@ -570,6 +613,8 @@ int sol_gpu_batch_destroy(SolGpuBatch* b) {
     cudaFree(b->d_adj_views);
     cudaFree(b->d_dc);
     cudaFree(b->scratch);
+    cudaFree(b->d_scene_box);
+    cudaFree(b->d_sort_bins);
     if (b->h_ctr) cudaFreeHost(b->h_ctr);
     if (b->capture) cudaStreamDestroy(b->capture);
     if (b->ev_start) cudaEventDestroy(b->ev_start);
@@ -726,28 +771,32 @@ int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const Sol
     for (auto& v : probe) { v.film = scratch + off; off += 3 * (size_t)v.width * v.height; v.sample_count = 1; }
     cudaStream_t s = b->capture;
     const uint32_t caps[] = {1u << 20, 1u << 21, 1u << 22, 1u << 23};
-    const uint32_t blocks[] = {64, 128, 256};
+    const uint32_t blocks[] = {128, 256};
     const uint32_t sorts[] = {0u, 1u << 16, 0xffffffffu};
+    const int32_t orders[] = {SOL_GPU_RAY_ORDER_QUEUE, SOL_GPU_RAY_ORDER_SORTED};
     float best_ms = 1e30f;
     int rc = SOL_GPU_OK;
     const SolGpuBatchOptions saved = b->opts;
     for (uint32_t cap : caps) {
         for (uint32_t blk : blocks) {
             for (uint32_t srt : sorts) {
-                b->opts.capacity = cap;
-                b->opts.block_size = blk;
-                b->opts.sort_threshold = srt;
-                float ms = 0.0f;
-                for (int rep = 0; rep < 2 && rc == SOL_GPU_OK; ++rep) {   // first run warms the graph
-                    rc = render_batch(b, config, probe.data(), num_views, s);
-                    if (rc == SOL_GPU_OK) {
-                        e = cudaEventSynchronize(b->ev_stop);
-                        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
-                        if (e != cudaSuccess) rc = cuda_fail(e, "autotune timing");
+                for (int32_t order : orders) {
+                    b->opts.capacity = cap;
+                    b->opts.block_size = blk;
+                    b->opts.sort_threshold = srt;
+                    b->opts.ray_order = order;
+                    float ms = 0.0f;
+                    for (int rep = 0; rep < 2 && rc == SOL_GPU_OK; ++rep) {   // first run warms the graph
+                        rc = render_batch(b, config, probe.data(), num_views, s);
+                        if (rc == SOL_GPU_OK) {
+                            e = cudaEventSynchronize(b->ev_stop);
+                            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, b->ev_start, b->ev_stop);
+                            if (e != cudaSuccess) rc = cuda_fail(e, "autotune timing");
+                        }
                     }
+                    if (rc != SOL_GPU_OK) break;
+                    if (ms < best_ms) { best_ms = ms; best = b->opts; }
                 }
-                if (rc != SOL_GPU_OK) break;
-                if (ms < best_ms) { best_ms = ms; best = b->opts; }
             }
         }
     }
@@ -777,7 +826,7 @@ int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const Sol
     if (cache_path) {
         std::ofstream f(cache_path, std::ios::app);
         f << key << '\t' << best.capacity << ' ' << best.block_size << ' ' << best.sort_threshold << ' '
-          << best.schedule << '\n';
+          << best.schedule << ' ' << best.ray_order << '\n';
     }
     return SOL_GPU_OK;
 }

@@ -390,6 +390,119 @@ wf_shadow(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable 
     if (lane_id() == 0 && rays) { atomicAdd(&ctr->rays, rays); atomicAdd(&ctr->shadow_rays, rays); }
 }
 
+/// Spreads the low 10 bits of x to every third bit.
+__device__ __forceinline__ uint32_t spread3(uint32_t x) {
+    x &= 0x3ffu;
+    x = (x | (x << 16)) & 0x030000ffu;
+    x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+/// Sort key of a ray (see kWfSortBits): scene index, direction octant, Morton
+/// cell of the origin in the scene's bounds, from the high bits down.
+__device__ __forceinline__ uint32_t ray_key(const WfParams& P, float4 o, float4 d, uint32_t scene) {
+    const int per = (kWfSortBits - 3 - (int)P.scene_bits) / 3;   // Morton bits per axis
+    const float cells = (float)(1u << per);
+    const float4 lo = P.scene_box[2 * scene], hi = P.scene_box[2 * scene + 1];
+    const float fx = fminf(fmaxf((o.x - lo.x) / fmaxf(hi.x - lo.x, 1e-20f), 0.0f), 0.999999f);
+    const float fy = fminf(fmaxf((o.y - lo.y) / fmaxf(hi.y - lo.y, 1e-20f), 0.0f), 0.999999f);
+    const float fz = fminf(fmaxf((o.z - lo.z) / fmaxf(hi.z - lo.z, 1e-20f), 0.0f), 0.999999f);
+    // NaN origins (none arise; they would compare false above) land in cell 0.
+    const uint32_t ix = fx == fx ? (uint32_t)(fx * cells) : 0u;
+    const uint32_t iy = fy == fy ? (uint32_t)(fy * cells) : 0u;
+    const uint32_t iz = fz == fz ? (uint32_t)(fz * cells) : 0u;
+    const uint32_t morton = spread3(ix) | (spread3(iy) << 1) | (spread3(iz) << 2);
+    const uint32_t octant = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+    const uint32_t key = (scene << (kWfSortBits - P.scene_bits)) | (octant << (3 * per)) | morton;
+    return key & (kWfSortBins - 1u);
+}
+
+/// Reordering, step 1: the key of every queued ray and the key histogram
+/// (per block in shared memory, then added to P.sort_bins).  `shadow`: the
+/// shadow queue (tag in the origin's w), else the extend queue of this
+/// iteration's parity (tag in the direction's w).
+__global__ void __launch_bounds__(1024) wf_sort_hist(const WfParams* __restrict__ Pp, int shadow) {
+    extern __shared__ uint32_t hist[];
+    const WfParams& P = *Pp;
+    const uint32_t p = P.ctr->iter & 1u;
+    const uint32_t n = shadow ? P.ctr->shadow : P.ctr->extend[p];
+    const float4* __restrict__ so = shadow ? P.sh_o : P.ray_o[p];
+    const float4* __restrict__ sd = shadow ? P.sh_d : P.ray_d[p];
+    for (uint32_t b = threadIdx.x; b < kWfSortBins; b += blockDim.x) hist[b] = 0u;
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 o = so[i], d = sd[i];
+        const uint32_t tag = __float_as_uint(shadow ? o.w : d.w);
+        const uint32_t key = ray_key(P, o, d, tag >> kWfSlotBits);
+        P.sort_key[i] = key;
+        atomicAdd(&hist[key], 1u);
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < kWfSortBins; b += blockDim.x)
+        if (hist[b]) atomicAdd(&P.sort_bins[b], hist[b]);
+}
+
+/// Reordering, step 2 (one block of 1024 threads): exclusive prefix sums of
+/// the histogram into the bins' offsets; the counts are cleared for the next use.
+__global__ void __launch_bounds__(1024) wf_sort_scan(const WfParams* __restrict__ Pp) {
+    __shared__ uint32_t part[1024];
+    const WfParams& P = *Pp;
+    constexpr uint32_t per = kWfSortBins / 1024;
+    const uint32_t t = threadIdx.x;
+    uint32_t local[per];
+    uint32_t sum = 0;
+    for (uint32_t k = 0; k < per; ++k) {
+        local[k] = P.sort_bins[t * per + k];
+        sum += local[k];
+    }
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {   // inclusive scan of the per-thread sums
+        const uint32_t v = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t at = part[t] - sum;
+    for (uint32_t k = 0; k < per; ++k) {
+        P.sort_bins[kWfSortBins + t * per + k] = at;
+        P.sort_bins[t * per + k] = 0u;
+        at += local[k];
+    }
+}
+
+/// Reordering, step 3: every ray moves to its bin's next place in the spare
+/// arrays (the order inside a bin is that of the atomics; results do not
+/// depend on it, only on each ray).
+__global__ void __launch_bounds__(256) wf_sort_scatter(const WfParams* __restrict__ Pp, int shadow) {
+    const WfParams& P = *Pp;
+    const uint32_t p = P.ctr->iter & 1u;
+    const uint32_t n = shadow ? P.ctr->shadow : P.ctr->extend[p];
+    const float4* __restrict__ so = shadow ? P.sh_o : P.ray_o[p];
+    const float4* __restrict__ sd = shadow ? P.sh_d : P.ray_d[p];
+    uint32_t* offsets = P.sort_bins + kWfSortBins;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t key = P.sort_key[i];
+        const uint32_t at = append_keyed(offsets, (int)key);
+        P.alt[0][at] = so[i];
+        P.alt[1][at] = sd[i];
+        if (shadow) P.alt[2][at] = P.sh_c[i];
+    }
+}
+
+/// Reordering, step 4 (one thread): the reordered arrays become the queue's,
+/// the queue's become the spares.
+__global__ void wf_sort_swap(WfParams* __restrict__ P, int shadow) {
+    const uint32_t p = P->ctr->iter & 1u;
+    float4*& o = shadow ? P->sh_o : P->ray_o[p];
+    float4*& d = shadow ? P->sh_d : P->ray_d[p];
+    float4* t = o; o = P->alt[0]; P->alt[0] = t;
+    t = d; d = P->alt[1]; P->alt[1] = t;
+    if (shadow) { t = P->sh_c; P->sh_c = P->alt[2]; P->alt[2] = t; }
+}
+
 /// Resets the consumed queues, flips the parity and sets the loop condition.
 __global__ void wf_advance(const WfParams* __restrict__ Pp, cudaGraphConditionalHandle handle, int use_handle) {
     const WfParams& P = *Pp;
@@ -450,12 +563,33 @@ cudaError_t launch_wf_init(const WfParams* params, uint32_t capacity, cudaStream
     return cudaGetLastError();
 }
 
-cudaError_t launch_wf_iteration(const WfParams* params, const WfSceneTable& scenes, bool basic, const WfLaunch& L,
-                                cudaGraphConditionalHandle handle, int use_handle, cudaStream_t stream) {
+namespace {
+
+/// The four reordering launches of one queue (see wf_sort_hist).
+void launch_sort(WfParams* params, int shadow, int sms, cudaStream_t stream) {
+    wf_sort_hist<<<2 * sms, 1024, kWfSortBins * sizeof(uint32_t), stream>>>(params, shadow);
+    wf_sort_scan<<<1, 1024, 0, stream>>>(params);
+    wf_sort_scatter<<<8 * sms, 256, 0, stream>>>(params, shadow);
+    wf_sort_swap<<<1, 1, 0, stream>>>(params, shadow);
+}
+
+}  // namespace
+
+cudaError_t allow_sort_smem() {
+    return cudaFuncSetAttribute(wf_sort_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(kWfSortBins * sizeof(uint32_t)));
+}
+
+cudaError_t launch_wf_iteration(WfParams* params, const WfSceneTable& scenes, bool basic, bool ray_sort,
+                                const WfLaunch& L, cudaGraphConditionalHandle handle, int use_handle,
+                                cudaStream_t stream) {
+    const int sms = L.sms > 0 ? L.sms : 1;
     wf_generate<<<L.grid[0], L.block[0], 0, stream>>>(params);
+    if (ray_sort) launch_sort(params, 0, sms, stream);
     wf_extend<<<L.grid[1], L.block[1], trace_smem(L.block[1]), stream>>>(params, scenes);
     if (basic) wf_shade<true><<<L.grid[2], L.block[2], 0, stream>>>(params, scenes);
     else wf_shade<false><<<L.grid[2], L.block[2], 0, stream>>>(params, scenes);
+    if (ray_sort) launch_sort(params, 1, sms, stream);
     wf_shadow<<<L.grid[3], L.block[3], trace_smem(L.block[3]), stream>>>(params, scenes);
     wf_advance<<<1, 1, 0, stream>>>(params, handle, use_handle);
     return cudaGetLastError();

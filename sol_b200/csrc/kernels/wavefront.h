@@ -48,6 +48,14 @@ struct WfSceneTable {
     SceneView v[kWfMaxScenes];
 };
 
+/// Ray reordering (SolGpuBatchOptions::ray_order = SOL_GPU_RAY_ORDER_SORTED):
+/// before each traversal stage the queue is counting-sorted by a key of
+/// kWfSortBits bits -- the ray's scene, the octant of its direction and the
+/// Morton cell of its origin in the scene's bounds -- so that neighbouring
+/// lanes start in the same part of the hierarchy.
+constexpr int kWfSortBits = 14;
+constexpr uint32_t kWfSortBins = 1u << kWfSortBits;
+
 /// One view of a batch: a constructed camera, its film and sample range.
 /// Work items are 8x4 pixel tiles of 32 items each; split views (every
 /// wavefront view, and the multi-view megakernel's views of more than one
@@ -104,6 +112,12 @@ struct WfParams {
     unsigned long long max_iterations;   // self-check bound on bounce-loop iterations
     int refill_below;        // a traversal warp refills its idle lanes when fewer than this many are busy
     uint32_t keep_counts;    // 1: add this launch's paths and rays to the counters instead of restarting them
+    uint32_t ray_sort;       // 1: reorder each ray queue before it is traced (see kWfSortBits)
+    uint32_t scene_bits;     // bits of the sort key taken by the scene index
+    const float4* scene_box; // per scene: lower corner, upper corner (2 float4)
+    uint32_t* sort_key;      // per queue position: the ray's key (scratch of the reordering)
+    uint32_t* sort_bins;     // kWfSortBins counts, then kWfSortBins offsets
+    float4* alt[3];          // spare queue arrays: reordered rays land here and swap places with the queue's
     DConfig cfg;
     const WfView* views;
     WfCounters* ctr;
@@ -127,6 +141,7 @@ struct WfParams {
 struct WfLaunch {
     int grid[4];
     int block[4];
+    int sms;                 // multiprocessors of the device (grids of the reordering kernels)
 };
 
 int wavefront_blocks_per_sm(int stage, int block);
@@ -134,7 +149,13 @@ cudaError_t launch_wf_init(const WfParams* params, uint32_t capacity, cudaStream
 /// One bounce of the wavefront: generate, extend, shade, shadow, advance.
 /// `basic`: every scene has basic shading (shade's build without image
 /// textures and Interp BSDFs).
-cudaError_t launch_wf_iteration(const WfParams* params, const WfSceneTable& scenes, bool basic, const WfLaunch& launch,
-                                cudaGraphConditionalHandle handle, int use_handle, cudaStream_t stream);
+/// `ray_sort`: reorder the extend and shadow queues before they are traced
+/// (WfParams::ray_sort must agree).  `params` is in device memory; the
+/// reordering swaps queue arrays in it.
+cudaError_t launch_wf_iteration(WfParams* params, const WfSceneTable& scenes, bool basic, bool ray_sort,
+                                const WfLaunch& launch, cudaGraphConditionalHandle handle, int use_handle,
+                                cudaStream_t stream);
+/// Lets the reordering's histogram kernel use kWfSortBins * 4 bytes of shared memory (current device).
+cudaError_t allow_sort_smem();
 
 }  // namespace sol_b200

@@ -260,10 +260,11 @@ class BatchRenderer:
     wavefront launch (sol_gpu_batch_*).  Films are device pointers (3*w*h floats)."""
 
     def __init__(self, scenes, capacity: int = 0, block_size: int = 0, sort_threshold: int = 0,
-                 host_loop: bool = False, schedule: int = capi.BATCH_WAVEFRONT):
+                 host_loop: bool = False, schedule: int = capi.BATCH_WAVEFRONT, ray_order: int = 0):
         self.scenes = list(scenes)
         arr = (capi.ScenePtr * len(self.scenes))(*[s.handle for s in self.scenes])
-        opts = capi.SolGpuBatchOptions(capacity, block_size, sort_threshold, int(host_loop), int(schedule))
+        opts = capi.SolGpuBatchOptions(capacity, block_size, sort_threshold, int(host_loop), int(schedule),
+                                       int(ray_order))
         h = capi.BatchPtr()
         capi.check(capi.lib.sol_gpu_batch_create(arr, len(self.scenes), C.byref(opts), C.byref(h)),
                    "sol_gpu_batch_create")

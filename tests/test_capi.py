@@ -31,7 +31,7 @@ def test_library_exports_every_header_function(built):
 
 def test_abi_version(built):
     from sol_b200 import capi
-    assert capi.lib.sol_gpu_abi_version() == 2
+    assert capi.lib.sol_gpu_abi_version() == 3
 
 
 def _create(scene):

@@ -50,6 +50,8 @@ def _render_both(scenes, specs, cfg, scratch_limit=0, **opts):
 
 @pytest.mark.parametrize("opts", [dict(), dict(capacity=4096, block_size=64), dict(sort_threshold=0xFFFFFFFF),
                                   dict(sort_threshold=0), dict(capacity=32, block_size=128),
+                                  dict(ray_order=1), dict(ray_order=2, sort_threshold=0),
+                                  dict(ray_order=2, host_loop=True, capacity=1000),
                                   dict(host_loop=True, block_size=256), dict(schedule=1),
                                   # scratch for about two samples of every view: the samples run in chunks
                                   dict(scratch_limit=2 * 3 * 4 * 96 * 96 * 12)])
