@@ -329,10 +329,11 @@ typedef struct SolGpuBatchOptions {
 } SolGpuBatchOptions;
 
 /* Order in which the wavefront traces each bounce's rays.  QUEUE: as the
- * stages queued them.  SORTED: counting-sorted first by scene, direction
- * octant and the Morton cell of the origin, so that neighbouring lanes walk
- * the same part of the hierarchy.  DEFAULT (0) is SORTED.  Films are the same
- * bits either way. */
+ * stages queued them (camera rays in 8x4 pixel tiles, bounce rays in their
+ * parents' order).  SORTED: counting-sorted first by scene, direction octant
+ * and the Morton cell of the origin (14-bit key).  DEFAULT (0) is QUEUE, which
+ * measured faster: the coarse cells lose the tiles' finer coherence.  Films
+ * are the same bits either way. */
 #define SOL_GPU_RAY_ORDER_DEFAULT 0
 #define SOL_GPU_RAY_ORDER_QUEUE   1
 #define SOL_GPU_RAY_ORDER_SORTED  2
@@ -379,7 +380,7 @@ int sol_gpu_batch_set_scratch_limit(SolGpuBatch* batch, uint64_t bytes);
 int sol_gpu_batch_set_iteration_limit(SolGpuBatch* batch, uint64_t max_iterations);
 
 /* Times candidate options (capacity, block size, binning threshold, ray order; with
- * schedule AUTO also the megakernel schedule) on one sample per pixel of the
+ * schedule AUTO also the megakernel schedule) on up to four samples per pixel of the
  * given views, rendered into scratch films, adopts the fastest and returns it
  * in `chosen`.  With `cache_path` set, a previous
  * choice for the same device and batch shape is read from that file instead,

@@ -434,7 +434,7 @@ int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVie
     rc = configure_launch(b);
     if (rc != SOL_GPU_OK) return rc;
     WfParams& h = b->host;
-    const bool ray_sort = b->opts.ray_order != SOL_GPU_RAY_ORDER_QUEUE;
+    const bool ray_sort = b->opts.ray_order == SOL_GPU_RAY_ORDER_SORTED;
     if (ray_sort != b->graph_sort) {
         destroy_graph(b);
         b->graph_sort = ray_sort;
@@ -768,9 +768,14 @@ int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const Sol
     cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&scratch), sizeof(float) * std::max<size_t>(floats, 1));
     if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc autotune films");
     size_t off = 0;
-    for (auto& v : probe) { v.film = scratch + off; off += 3 * (size_t)v.width * v.height; v.sample_count = 1; }
+    // Up to four samples per pixel: enough work items that the pool sizes differ.
+    for (auto& v : probe) {
+        v.film = scratch + off;
+        off += 3 * (size_t)v.width * v.height;
+        v.sample_count = std::min<uint32_t>(v.sample_count, 4);
+    }
     cudaStream_t s = b->capture;
-    const uint32_t caps[] = {1u << 20, 1u << 21, 1u << 22, 1u << 23};
+    const uint32_t caps[] = {1u << 21, 1u << 22, 1u << 23, 1u << 24};
     const uint32_t blocks[] = {128, 256};
     const uint32_t sorts[] = {0u, 1u << 16, 0xffffffffu};
     const int32_t orders[] = {SOL_GPU_RAY_ORDER_QUEUE, SOL_GPU_RAY_ORDER_SORTED};

@@ -52,7 +52,10 @@ struct WfSceneTable {
 /// before each traversal stage the queue is counting-sorted by a key of
 /// kWfSortBits bits -- the ray's scene, the octant of its direction and the
 /// Morton cell of its origin in the scene's bounds -- so that neighbouring
-/// lanes start in the same part of the hierarchy.
+/// lanes start in the same part of the hierarchy.  Measured slower than the
+/// queue's own order (64 views: 725 against 789 Mpaths/s; 32 scenes: 1823
+/// against 2221): the cells are coarse and the scatter shuffles rays inside a
+/// cell, losing the pixel tiles' coherence; off by default.
 constexpr int kWfSortBits = 14;
 constexpr uint32_t kWfSortBins = 1u << kWfSortBits;
 
