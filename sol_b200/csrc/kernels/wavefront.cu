@@ -124,6 +124,21 @@ __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ 
     const uint32_t n = ctr->ended[p];
     const uint32_t total = P.total_items;
     unsigned long long paths = 0;
+#if SOL_WF_GEN_SMEM_VIEWS
+    // The view table in shared memory when it is small: the claim loop's
+    // binary search and the view fields then cost no global round trips.
+    __shared__ uint4 view_smem[kGenSmemViews * sizeof(WfView) / sizeof(uint4)];
+    const WfView* views = P.views;
+    if (P.num_views <= kGenSmemViews) {
+        const uint4* src = reinterpret_cast<const uint4*>(P.views);
+        const uint32_t words = P.num_views * (uint32_t)(sizeof(WfView) / sizeof(uint4));
+        for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) view_smem[w] = src[w];
+        views = reinterpret_cast<const WfView*>(view_smem);
+    }
+    __syncthreads();
+#else
+    const WfView* views = P.views;
+#endif
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t i = base + threadIdx.x;
         if (i >= n) continue;
@@ -134,14 +149,14 @@ __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ 
         while (true) {
             if (it.x != kIdle) {
                 // path_tracer.cpp:19 -- the pixel's sum is formed by the sum pass
-                reinterpret_cast<float4*>(P.views[it.x].scratch)[it.y] = make_float4(col.x, col.y, col.z, 0.0f);
+                reinterpret_cast<float4*>(views[it.x].scratch)[it.y] = make_float4(col.x, col.y, col.z, 0.0f);
                 it.x = kIdle;
             }
             if (++claims > total + 2u) { atomicOr(&ctr->error, kFaultClaimLoop); break; }
             const uint32_t item = append(&ctr->next_item);
             if (item >= total) break;
-            const uint32_t vi = find_view(P.views, P.num_views, item);
-            const WfView& v = P.views[vi];
+            const uint32_t vi = find_view(views, P.num_views, item);
+            const WfView& v = views[vi];
             const uint32_t per_sample = v.tiles_x * ((v.height + 3u) / 4u) * 32u;
             const uint32_t local = item - v.item_begin;
             const uint32_t k = local / per_sample;
@@ -298,7 +313,7 @@ wf_extend(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable 
 
 /// K5: SoL's per-vertex step for every closest hit (kind by kind when binned).
 template <bool kBasic>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, kWfShadeMinBlocks)
 wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable scenes) {
     const WfParams& P = *Pp;
     WfCounters* ctr = P.ctr;

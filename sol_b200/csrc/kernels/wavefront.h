@@ -26,6 +26,19 @@ constexpr int kWfRefillBelow = SOL_WF_REFILL_BELOW;
 /// Resident 256-thread blocks per SM the traversal stages' registers must allow.
 constexpr int kWfTraceMinBlocks = SOL_WF_TRACE_MIN_BLOCKS;
 
+#ifndef SOL_WF_SHADE_MIN_BLOCKS
+#define SOL_WF_SHADE_MIN_BLOCKS 3
+#endif
+/// Resident 256-thread blocks per SM the shading stage's registers must allow.
+constexpr int kWfShadeMinBlocks = SOL_WF_SHADE_MIN_BLOCKS;
+
+#ifndef SOL_WF_GEN_SMEM_VIEWS
+#define SOL_WF_GEN_SMEM_VIEWS 1
+#endif
+/// The generate stage copies view tables of up to this many views into shared
+/// memory (SOL_WF_GEN_SMEM_VIEWS=0: reads them from global memory).
+constexpr uint32_t kGenSmemViews = 64;
+
 #ifndef SOL_WF_SHARED_STACK
 #define SOL_WF_SHARED_STACK 0
 #endif
@@ -86,6 +99,8 @@ struct WfView {
     uint32_t first_chunk;    // the sum starts from 0 (else from `running`)
     uint32_t last_chunk;     // the sum goes into the film (else into `running`)
 };
+
+static_assert(sizeof(WfView) % 16 == 0, "the generate stage copies views as 16-byte words");
 
 struct WfCounters {
     uint32_t extend[2];      // rays queued for the closest-hit stage, by parity
