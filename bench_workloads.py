@@ -216,7 +216,9 @@ def run_cornell(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=Tru
     import torch
     from sol_b200 import scenes
     from sol_b200.renderer import GpuPathTracer, GpuScene, Image
-    steps = steps or args.steps
+    # A render takes about 2 ms: at least 200 timed steps, so that the clock
+    # sampler (one sample per 100 ms) sees the timed region.
+    steps = max(steps or args.steps, 200)
     warmup = warmup or args.warmup
     scene, cfg, w, h, spp = scenes.cornell_frame()
     gs = GpuScene(scene)
