@@ -20,6 +20,9 @@ namespace sol_b200 {
 #ifndef SOL_MEGAKERNEL_SMALL_MIN_BLOCKS
 #define SOL_MEGAKERNEL_SMALL_MIN_BLOCKS 12   // 40 registers: renders of a few paths per lane, where spills cost more
 #endif
+#ifndef SOL_MEGAKERNEL_SPLIT_LEAN
+#define SOL_MEGAKERNEL_SPLIT_LEAN 1   // 1: the split schedule's lean kernel (pt_megakernel_lean)
+#endif
 #ifndef SOL_MEGAKERNEL_SHARED_STACK
 #define SOL_MEGAKERNEL_SHARED_STACK 0   // 1: first traversal-stack entries in shared memory (measured 5% slower)
 #endif

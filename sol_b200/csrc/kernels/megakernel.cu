@@ -169,6 +169,73 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
     }
 }
 
+/// K1 in the split schedule, lean form: every work item is one path, so a lane
+/// claims an item, traces its path to the end and writes the colour (0 +
+/// colour, as the per-pixel sum starts) to the scratch plane of its sample,
+/// then claims the next.  The same path computation and the same scratch as
+/// pt_megakernel<kCount = false, kSplit = true>, with less state live across
+/// the traversal (no per-pixel sum, sample range or loop bounds: the claim
+/// loop ends with the items and the bounce loop with the path length, and
+/// the traversal keeps its own step bound), so the 32-register build spills
+/// less.
+template <int kMinBlocks, bool kBasic>
+__global__ void __launch_bounds__(kMegakernelBlock, kMinBlocks)
+pt_megakernel_lean(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint32_t sample_count,
+                   uint32_t width, uint32_t height, float* __restrict__ scratch, DeviceCounters* __restrict__ ctr) {
+    const uint32_t tiles_x = (width + 7u) / 8u;
+    const uint32_t total = tiles_x * ((height + 3u) / 4u) * 32u;   // items of one sample
+    const uint32_t items = total * sample_count;
+    const size_t plane = (size_t)width * height;
+    const float light_pick_prob = 1.0f / (float)s.num_lights;
+    TraversalCounters tc{0u, 0u};
+    uint32_t n_paths = 0, n_rays = 0, n_shadow = 0;
+    LocalStack stack;
+    while (true) {
+        const uint32_t item = claim_items(&ctr->next_item);
+        if (item >= items) break;
+        const uint32_t k = item / total;
+        const uint32_t it = item - k * total;
+        const uint32_t tile = it >> 5, l = it & 31u;
+        const uint32_t px = (tile % tiles_x) * 8u + (l & 7u);
+        const uint32_t py = (tile / tiles_x) * 4u + (l >> 3);
+        if (px >= width || py >= height) continue;   // padding of a partial tile
+        PathState ps;
+        start_path(ps, cam, sample_index + k, px, py, width, height);
+        ++n_paths;
+        while (ps.path_len < cfg.max_path_len) {
+            // closest hit (path_tracer.cpp:42)
+            float t = kFloatMax;
+            const int slot = traverse<false, false>(s, ps.org, ps.dir, ps.tmin, t, tc, stack);
+            ++n_rays;
+            if (slot < 0) break;
+            VertexOut vo;
+            shade_vertex<kBasic>(s, cfg, light_pick_prob, slot, t, ps, vo);
+            // shadow ray of this vertex (path_tracer.cpp:72-74)
+            if (vo.has_shadow) {
+                float smax = 1.0f - cfg.ray_offset;
+                const int occ = traverse<true, false>(s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc, stack);
+                ++n_rays;
+                ++n_shadow;
+                if (occ < 0) ps.color = ps.color + vo.pending;
+            }
+            if (vo.end) break;
+            ++ps.path_len;
+        }
+        const Rgb c = rgb(0.0f) + ps.color;   // path_tracer.cpp:19, the sum pass adds the rest in sample order
+        float* f = scratch + (size_t)k * 3u * plane + (size_t)py * width + px;
+        f[0] = c.r;
+        f[plane] = c.g;
+        f[2 * plane] = c.b;
+    }
+    __syncwarp();
+    unsigned long long v0 = warp_sum_u64(n_paths), v1 = warp_sum_u64(n_rays), v2 = warp_sum_u64(n_shadow);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&ctr->paths, v0);
+        atomicAdd(&ctr->rays, v1);
+        atomicAdd(&ctr->shadow_rays, v2);
+    }
+}
+
 /// K1b: the megakernel over many views (cameras, films of uneven size and spp)
 /// of one or more scenes in one persistent launch.  Work items are the views'
 /// 8x4 pixel tiles laid end to end (WfView::item_begin); a lane claims a pixel
@@ -354,6 +421,14 @@ template <bool kSplit>
 auto megakernel_fn(bool instrumented, bool full, bool basic) {
     if (instrumented) return full ? pt_megakernel<true, kSplit, kMegakernelMinBlocks, false>
                                   : pt_megakernel<true, kSplit, kMegakernelSmallMinBlocks, false>;
+#if SOL_MEGAKERNEL_SPLIT_LEAN
+    if (kSplit) {
+        if (basic) return full ? pt_megakernel_lean<kMegakernelMinBlocks, true>
+                               : pt_megakernel_lean<kMegakernelSmallMinBlocks, true>;
+        return full ? pt_megakernel_lean<kMegakernelMinBlocks, false>
+                    : pt_megakernel_lean<kMegakernelSmallMinBlocks, false>;
+    }
+#endif
     if (basic) return full ? pt_megakernel<false, kSplit, kMegakernelMinBlocks, true>
                            : pt_megakernel<false, kSplit, kMegakernelSmallMinBlocks, true>;
     return full ? pt_megakernel<false, kSplit, kMegakernelMinBlocks, false>
