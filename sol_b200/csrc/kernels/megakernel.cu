@@ -169,24 +169,6 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
     }
 }
 
-/// Pixel and sample of split-schedule work item `item` (items sample-major,
-/// 8x4 pixel tiles of 32 items, `total` items per sample).
-__device__ __forceinline__ void item_pixel(uint32_t item, uint32_t total, uint32_t tiles_x, uint32_t* px,
-                                           uint32_t* py, uint32_t* k) {
-    *k = item / total;
-    const uint32_t it = item - *k * total;
-    const uint32_t tile = it >> 5, l = it & 31u;
-    *px = (tile % tiles_x) * 8u + (l & 7u);
-    *py = (tile / tiles_x) * 4u + (l >> 3);
-}
-
-/// Adds the number of calling lanes of the warp to a shared counter (one
-/// shared-memory atomic per warp).
-__device__ __forceinline__ void count_warp(unsigned long long* counter) {
-    const unsigned mask = __activemask();
-    if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) atomicAdd(counter, (unsigned long long)__popc(mask));
-}
-
 /// K1 in the split schedule, lean form: every work item is one path, so a lane
 /// claims an item, traces its path to the end and writes the colour (0 +
 /// colour, as the per-pixel sum starts) to the scratch plane of its sample,
@@ -200,57 +182,57 @@ template <int kMinBlocks, bool kBasic>
 __global__ void __launch_bounds__(kMegakernelBlock, kMinBlocks)
 pt_megakernel_lean(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint32_t sample_count,
                    uint32_t width, uint32_t height, float* __restrict__ scratch, DeviceCounters* __restrict__ ctr) {
-    // Ray and path counts go to the block's shared counters, a warp at a time,
-    // so that no counter register lives across the traversal.
-    __shared__ unsigned long long blk_paths, blk_rays, blk_shadow;
-    if (threadIdx.x == 0) blk_paths = blk_rays = blk_shadow = 0ull;
-    __syncthreads();
     const uint32_t tiles_x = (width + 7u) / 8u;
     const uint32_t total = tiles_x * ((height + 3u) / 4u) * 32u;   // items of one sample
     const uint32_t items = total * sample_count;
+    const size_t plane = (size_t)width * height;
+    const float light_pick_prob = 1.0f / (float)s.num_lights;
     TraversalCounters tc{0u, 0u};
+    uint32_t n_paths = 0, n_rays = 0, n_shadow = 0;
     LocalStack stack;
     while (true) {
         const uint32_t item = claim_items(&ctr->next_item);
         if (item >= items) break;
-        uint32_t px, py, k;
-        item_pixel(item, total, tiles_x, &px, &py, &k);
+        const uint32_t k = item / total;
+        const uint32_t it = item - k * total;
+        const uint32_t tile = it >> 5, l = it & 31u;
+        const uint32_t px = (tile % tiles_x) * 8u + (l & 7u);
+        const uint32_t py = (tile / tiles_x) * 4u + (l >> 3);
         if (px >= width || py >= height) continue;   // padding of a partial tile
         PathState ps;
         start_path(ps, cam, sample_index + k, px, py, width, height);
-        count_warp(&blk_paths);
+        ++n_paths;
         while (ps.path_len < cfg.max_path_len) {
             // closest hit (path_tracer.cpp:42)
             float t = kFloatMax;
             const int slot = traverse<false, false>(s, ps.org, ps.dir, ps.tmin, t, tc, stack);
-            count_warp(&blk_rays);
+            ++n_rays;
             if (slot < 0) break;
             VertexOut vo;
-            shade_vertex<kBasic>(s, cfg, 1.0f / (float)s.num_lights, slot, t, ps, vo);
+            shade_vertex<kBasic>(s, cfg, light_pick_prob, slot, t, ps, vo);
             // shadow ray of this vertex (path_tracer.cpp:72-74)
             if (vo.has_shadow) {
                 float smax = 1.0f - cfg.ray_offset;
                 const int occ = traverse<true, false>(s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc, stack);
-                count_warp(&blk_shadow);
+                ++n_rays;
+                ++n_shadow;
                 if (occ < 0) ps.color = ps.color + vo.pending;
             }
             if (vo.end) break;
             ++ps.path_len;
         }
-        // The pixel again from the item (three fewer registers across the path).
-        item_pixel(item, total, tiles_x, &px, &py, &k);
-        const size_t plane = (size_t)width * height;
         const Rgb c = rgb(0.0f) + ps.color;   // path_tracer.cpp:19, the sum pass adds the rest in sample order
         float* f = scratch + (size_t)k * 3u * plane + (size_t)py * width + px;
         f[0] = c.r;
         f[plane] = c.g;
         f[2 * plane] = c.b;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        atomicAdd(&ctr->paths, blk_paths);
-        atomicAdd(&ctr->rays, blk_rays + blk_shadow);
-        atomicAdd(&ctr->shadow_rays, blk_shadow);
+    __syncwarp();
+    unsigned long long v0 = warp_sum_u64(n_paths), v1 = warp_sum_u64(n_rays), v2 = warp_sum_u64(n_shadow);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&ctr->paths, v0);
+        atomicAdd(&ctr->rays, v1);
+        atomicAdd(&ctr->shadow_rays, v2);
     }
 }
 
