@@ -168,8 +168,7 @@ constexpr uint64_t kViewsScratchMaxBytes = uint64_t(4) << 30;
 /// order while their scratch fits in kViewsScratchMaxBytes; `sum_floats`
 /// receives the size of their sum pass.
 int upload_views(SolGpuBatch* b, const SolGpuView* views, uint32_t n, uint32_t* total_items, uint64_t* pixels,
-                 cudaStream_t stream, bool megakernel = false, uint64_t* sum_floats = nullptr,
-                 bool* one_path = nullptr) {
+                 cudaStream_t stream, bool megakernel = false, uint64_t* sum_floats = nullptr) {
     std::vector<WfView> v(n);
     uint64_t items = 0, px = 0;
     std::vector<uint64_t> scratch_at(n, 0);
@@ -235,11 +234,6 @@ int upload_views(SolGpuBatch* b, const SolGpuView* views, uint32_t n, uint32_t* 
     *total_items = (uint32_t)items;
     *pixels = px;
     if (sum_floats) *sum_floats = sum_at;
-    if (one_path) {
-        *one_path = true;
-        for (uint32_t i = 0; i < n; ++i)
-            if (views[i].sample_count > 1 && !v[i].split) *one_path = false;
-    }
     return SOL_GPU_OK;
 }
 
@@ -272,8 +266,7 @@ int render_megakernel(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVi
                       cudaStream_t stream) {
     uint32_t total_items = 0;
     uint64_t pixels = 0, sum_floats = 0;
-    bool one_path_views = false;
-    int rc = upload_views(b, views, n, &total_items, &pixels, stream, true, &sum_floats, &one_path_views);
+    int rc = upload_views(b, views, n, &total_items, &pixels, stream, true, &sum_floats);
     if (rc != SOL_GPU_OK) return rc;
     {
         if (!b->d_dc) {
@@ -283,8 +276,6 @@ int render_megakernel(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVi
         uint32_t max_spp = 0;
         for (uint32_t i = 0; i < n; ++i) max_spp = std::max(max_spp, views[i].sample_count);
         const int per_sm = megakernel_views_blocks_per_sm();
-        // Every work item is one path when every view of more than one sample was split.
-        const bool one_path = one_path_views;
         if (per_sm <= 0) return fail(SOL_GPU_ERR_CUDA, "megakernel occupancy query failed");
         cudaError_t e = cudaMemsetAsync(b->d_dc, 0, sizeof(DeviceCounters), stream);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
@@ -293,7 +284,7 @@ int render_megakernel(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVi
             const bool basic = std::all_of(b->scenes.begin(), b->scenes.end(),
                                            [](const SolGpuScene* s) { return s->basic_shading; });
             e = launch_megakernel_views(b->d_views, n, total_items, max_spp, b->d_scenes, b->h_scenes.data(),
-                                        (uint32_t)b->h_scenes.size(), basic, one_path, to_config(*config), b->d_dc,
+                                        (uint32_t)b->h_scenes.size(), basic, to_config(*config), b->d_dc,
                                         b->scenes[0]->fault, per_sm * b->num_sms, stream,
                                         b->scenes.size() == 1 ? b->scenes[0]->l2 : L2Window{});
             if (e == cudaSuccess) e = launch_sum_samples_views(b->d_views, n, sum_floats, stream);

@@ -100,12 +100,10 @@ int megakernel_views_blocks_per_sm();
 /// the same `num_scenes` views on the host: up to kViewsTableScenes of them go
 /// to the kernel by value (SceneTable), more are read from `scenes`.  `basic`:
 /// every scene has basic shading (no image textures, no Interp BSDFs).
-/// `one_path_items`: every view is split or has one sample, so every work
-/// item is one path (the lean kernel applies).
 cudaError_t launch_megakernel_views(const WfView* views, uint32_t num_views, uint32_t total_items, uint32_t max_spp,
                                     const SceneView* scenes, const SceneView* host_scenes, uint32_t num_scenes,
-                                    bool basic, bool one_path_items, const DConfig& cfg, DeviceCounters* counters,
-                                    unsigned int* fault, int grid, cudaStream_t stream, const L2Window& l2 = {});
+                                    bool basic, const DConfig& cfg, DeviceCounters* counters, unsigned int* fault,
+                                    int grid, cudaStream_t stream, const L2Window& l2 = {});
 
 /// Sum pass of the split views of launch_megakernel_views (see WfView::split).
 cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, uint64_t total_floats,

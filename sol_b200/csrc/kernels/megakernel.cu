@@ -371,91 +371,6 @@ pt_megakernel_views(const WfView* __restrict__ views, uint32_t num_views, uint32
     }
 }
 
-/// K1b, lean form, for batches whose every work item is one path (every view
-/// either split into (sample, pixel) items or of one sample): a lane claims an
-/// item of any view, traces its path and writes 0 + colour to the view's
-/// scratch plane of that sample (split views) or adds it into the film (one
-/// sample per pixel: the per-pixel sum 0 + colour, then the film's +=).  Same
-/// bits as pt_megakernel_views, with less state live across the traversal.
-template <bool kTable, bool kBasic>
-__global__ void __launch_bounds__(kMegakernelBlock, kMegakernelMinBlocks)
-pt_megakernel_views_lean(const WfView* __restrict__ views, uint32_t num_views, uint32_t total, uint32_t,
-                         const SceneView* __restrict__ scenes, const __grid_constant__ SceneTable table, DConfig cfg,
-                         DeviceCounters* __restrict__ ctr, unsigned int*) {
-    TraversalCounters tc{0u, 0u};
-    uint32_t n_paths = 0, n_rays = 0, n_shadow = 0;
-    LocalStack stack;
-    uint32_t vi = 0;
-    while (true) {
-        const uint32_t item = claim_items(&ctr->next_item);
-        if (item >= total) break;
-        // Consecutive claims almost always stay in the lane's current view.
-        uint32_t lo = vi;
-        if (!(views[vi].item_begin <= item && (vi + 1u == num_views || item < views[vi + 1u].item_begin))) {
-            lo = 0;
-            uint32_t hi = num_views;
-            while (hi - lo > 1) { const uint32_t mid = (lo + hi) >> 1; if (views[mid].item_begin <= item) lo = mid; else hi = mid; }
-        }
-        vi = lo;
-        const WfView& W = views[lo];
-        uint32_t local = item - W.item_begin, k = 0;
-        if (W.split) {
-            const uint32_t per_sample = W.tiles_x * ((W.height + 3u) / 4u) * 32u;
-            k = local / per_sample;
-            local -= k * per_sample;
-        }
-        const uint32_t tile = local >> 5, l = local & 31u;
-        const uint32_t px = (tile % W.tiles_x) * 8u + (l & 7u);
-        const uint32_t py = (tile / W.tiles_x) * 4u + (l >> 3);
-        if (px >= W.width || py >= W.height) continue;   // padding of a partial tile
-        const SceneView& s = kTable ? table.v[W.scene] : scenes[W.scene];
-        DCamera cam;
-        for (int c = 0; c < 3; ++c) { cam.eye[c] = W.eye[c]; cam.dir[c] = W.dir[c]; cam.right[c] = W.right[c]; cam.up[c] = W.up[c]; }
-        PathState ps;
-        start_path(ps, cam, W.sample_index + k, px, py, W.width, W.height);
-        ++n_paths;
-        while (ps.path_len < cfg.max_path_len) {
-            float t = kFloatMax;
-            const int slot = traverse<false, false>(s, ps.org, ps.dir, ps.tmin, t, tc, stack);
-            ++n_rays;
-            if (slot < 0) break;
-            VertexOut vo;
-            shade_vertex<kBasic>(s, cfg, 1.0f / (float)s.num_lights, slot, t, ps, vo);
-            if (vo.has_shadow) {
-                float smax = 1.0f - cfg.ray_offset;
-                const int occ = traverse<true, false>(s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc, stack);
-                ++n_rays;
-                ++n_shadow;
-                if (occ < 0) ps.color = ps.color + vo.pending;
-            }
-            if (vo.end) break;
-            ++ps.path_len;
-        }
-        const WfView& V = views[vi];
-        const size_t plane = (size_t)V.width * V.height;
-        const size_t i = (size_t)py * V.width + px;
-        const Rgb c = rgb(0.0f) + ps.color;   // path_tracer.cpp:19
-        if (V.split) {
-            float* f = V.scratch + (size_t)k * 3u * plane;
-            f[i] = c.r;
-            f[i + plane] = c.g;
-            f[i + 2 * plane] = c.b;
-        } else {
-            // image.h:54-60 accumulate (one sample per pixel in this launch)
-            V.film[i] += c.r;
-            V.film[i + plane] += c.g;
-            V.film[i + 2 * plane] += c.b;
-        }
-    }
-    __syncwarp();
-    unsigned long long v0 = warp_sum_u64(n_paths), v1 = warp_sum_u64(n_rays), v2 = warp_sum_u64(n_shadow);
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&ctr->paths, v0);
-        atomicAdd(&ctr->rays, v1);
-        atomicAdd(&ctr->shadow_rays, v2);
-    }
-}
-
 /// Adds each pixel's per-sample colours of one chunk of samples (scratch:
 /// sample_count x 3 planes) in sample order to the pixel's running sum, which
 /// starts from 0 with the first chunk as the per-pixel loop's sum does; after
@@ -546,20 +461,17 @@ int megakernel_views_blocks_per_sm() {
 
 cudaError_t launch_megakernel_views(const WfView* views, uint32_t num_views, uint32_t total_items, uint32_t max_spp,
                                     const SceneView* scenes, const SceneView* host_scenes, uint32_t num_scenes,
-                                    bool basic, bool one_path_items, const DConfig& cfg, DeviceCounters* counters,
-                                    unsigned int* fault, int grid, cudaStream_t stream, const L2Window& l2) {
+                                    bool basic, const DConfig& cfg, DeviceCounters* counters, unsigned int* fault,
+                                    int grid, cudaStream_t stream, const L2Window& l2) {
     SceneTable table{};
-    const bool lean = one_path_items && SOL_MEGAKERNEL_SPLIT_LEAN;
     if (num_scenes <= kViewsTableScenes) {
         for (uint32_t i = 0; i < num_scenes; ++i) table.v[i] = host_scenes[i];
-        auto fn = lean ? (basic ? pt_megakernel_views_lean<true, true> : pt_megakernel_views_lean<true, false>)
-                       : (basic ? pt_megakernel_views<false, true, true> : pt_megakernel_views<false, true, false>);
-        return launch_l2(fn, grid, kMegakernelBlock, 0, stream, l2, views, num_views, total_items, max_spp, scenes,
-                         table, cfg, counters, fault);
+        return launch_l2(basic ? pt_megakernel_views<false, true, true> : pt_megakernel_views<false, true, false>,
+                         grid, kMegakernelBlock, 0, stream, l2, views, num_views, total_items, max_spp, scenes, table,
+                         cfg, counters, fault);
     }
-    return launch_l2(lean ? pt_megakernel_views_lean<false, false> : pt_megakernel_views<false, false, false>, grid,
-                     kMegakernelBlock, 0, stream, l2, views, num_views, total_items, max_spp, scenes, table, cfg,
-                     counters, fault);
+    return launch_l2(pt_megakernel_views<false, false, false>, grid, kMegakernelBlock, 0, stream, l2, views, num_views,
+                     total_items, max_spp, scenes, table, cfg, counters, fault);
 }
 
 cudaError_t launch_sum_samples_views(const WfView* views, uint32_t num_views, uint64_t total_floats,
