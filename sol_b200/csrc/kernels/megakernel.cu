@@ -250,7 +250,7 @@ pt_megakernel_lean(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index,
 /// space as K1's scene is, so the traversal reads array pointers and sizes as
 /// constant operands; otherwise from the device array `scenes`.
 template <bool kCount, bool kTable, bool kBasic>
-__global__ void __launch_bounds__(kMegakernelBlock, kMegakernelMinBlocks)
+__global__ void __launch_bounds__(kMegakernelBlock, kMegakernelViewsMinBlocks)
 pt_megakernel_views(const WfView* __restrict__ views, uint32_t num_views, uint32_t total, uint32_t max_spp,
                     const SceneView* __restrict__ scenes, const __grid_constant__ SceneTable table, DConfig cfg,
                     DeviceCounters* __restrict__ ctr, unsigned int* __restrict__ fault) {
