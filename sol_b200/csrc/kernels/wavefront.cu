@@ -115,14 +115,62 @@ __global__ void __launch_bounds__(256) wf_init(const WfParams* __restrict__ Pp) 
     }
 }
 
-/// K2: ended paths write their colour to the scratch of their work item;
-/// their slots claim the next work items and start the camera rays.
+/// Ends the path of `slot` (colour `col` to the scratch of its work item) and
+/// starts the slot's next path: claims work items until one is a pixel, writes
+/// the new path's state and appends its camera ray to extend queue `qp`.  A
+/// slot that finds no item left goes idle.  Returns the paths started (0 or
+/// more: paths of length 0 end at once with a black colour).
+__device__ __forceinline__ uint32_t restart_slot(const WfParams& P, const WfView* views, uint32_t slot, float4 col,
+                                                 uint32_t qp) {
+    WfCounters* ctr = P.ctr;
+    const uint32_t total = P.total_items;
+    uint2 it = P.item[slot];
+    uint32_t claims = 0, paths = 0;
+    while (true) {
+        if (it.x != kIdle) {
+            // path_tracer.cpp:19 -- the pixel's sum is formed by the sum pass
+            reinterpret_cast<float4*>(views[it.x].scratch)[it.y] = make_float4(col.x, col.y, col.z, 0.0f);
+            it.x = kIdle;
+        }
+        if (++claims > total + 2u) { atomicOr(&ctr->error, kFaultClaimLoop); break; }
+        const uint32_t item = append(&ctr->next_item);
+        if (item >= total) break;
+        const uint32_t vi = find_view(views, P.num_views, item);
+        const WfView& v = views[vi];
+        const uint32_t per_sample = v.tiles_x * ((v.height + 3u) / 4u) * 32u;
+        const uint32_t local = item - v.item_begin;
+        const uint32_t k = local / per_sample;
+        const uint32_t in_sample = local - k * per_sample;
+        const uint32_t tile = in_sample >> 5, l = in_sample & 31u;
+        const uint32_t x = (tile % v.tiles_x) * 8u + (l & 7u);
+        const uint32_t y = (tile / v.tiles_x) * 4u + (l >> 3);
+        if (x >= v.width || y >= v.height) continue;   // padding of a partial tile: no pixel
+        PathState ps;
+        start_path(ps, view_camera(v), v.sample_index + k, x, y, v.width, v.height);
+        ++paths;
+        it = make_uint2(vi, local);
+        col = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (P.cfg.max_path_len == 0) continue;   // empty path: black, written above
+        P.thru[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        P.color[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
+        P.rng[slot] = ps.rng.state;
+        const uint32_t q = append(&ctr->extend[qp]);
+        P.ray_o[qp][q] = make_float4(ps.org.x, ps.org.y, ps.org.z, ps.tmin);
+        P.ray_d[qp][q] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, tag_bits(slot, v.scene));
+        break;
+    }
+    P.item[slot] = it;
+    return paths;
+}
+
+/// K2: the slots on the ended list (all slots at the start; later, the paths
+/// that ended after their last shadow ray, and with SOL_WF_SHADE_RESTART off
+/// every ended path) restart: colour out, next work item in.
 __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ Pp) {
     const WfParams& P = *Pp;
     WfCounters* ctr = P.ctr;
     const uint32_t p = ctr->iter & 1u;
     const uint32_t n = ctr->ended[p];
-    const uint32_t total = P.total_items;
     unsigned long long paths = 0;
 #if SOL_WF_GEN_SMEM_VIEWS
     // The view table in shared memory when it is small: the claim loop's
@@ -143,43 +191,7 @@ __global__ void __launch_bounds__(256) wf_generate(const WfParams* __restrict__ 
         const uint32_t i = base + threadIdx.x;
         if (i >= n) continue;
         const uint32_t slot = P.q_ended[p][i];
-        uint2 it = P.item[slot];
-        float4 col = P.color[slot];
-        uint32_t claims = 0;
-        while (true) {
-            if (it.x != kIdle) {
-                // path_tracer.cpp:19 -- the pixel's sum is formed by the sum pass
-                reinterpret_cast<float4*>(views[it.x].scratch)[it.y] = make_float4(col.x, col.y, col.z, 0.0f);
-                it.x = kIdle;
-            }
-            if (++claims > total + 2u) { atomicOr(&ctr->error, kFaultClaimLoop); break; }
-            const uint32_t item = append(&ctr->next_item);
-            if (item >= total) break;
-            const uint32_t vi = find_view(views, P.num_views, item);
-            const WfView& v = views[vi];
-            const uint32_t per_sample = v.tiles_x * ((v.height + 3u) / 4u) * 32u;
-            const uint32_t local = item - v.item_begin;
-            const uint32_t k = local / per_sample;
-            const uint32_t in_sample = local - k * per_sample;
-            const uint32_t tile = in_sample >> 5, l = in_sample & 31u;
-            const uint32_t x = (tile % v.tiles_x) * 8u + (l & 7u);
-            const uint32_t y = (tile / v.tiles_x) * 4u + (l >> 3);
-            if (x >= v.width || y >= v.height) continue;   // padding of a partial tile: no pixel
-            PathState ps;
-            start_path(ps, view_camera(v), v.sample_index + k, x, y, v.width, v.height);
-            ++paths;
-            it = make_uint2(vi, local);
-            col = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (P.cfg.max_path_len == 0) continue;   // empty path: black, written above
-            P.thru[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-            P.color[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
-            P.rng[slot] = ps.rng.state;
-            const uint32_t q = append(&ctr->extend[p]);
-            P.ray_o[p][q] = make_float4(ps.org.x, ps.org.y, ps.org.z, ps.tmin);
-            P.ray_d[p][q] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, tag_bits(slot, v.scene));
-            break;
-        }
-        P.item[slot] = it;
+        paths += restart_slot(P, views, slot, P.color[slot], p);
     }
     paths = warp_sum(paths);
     if (lane_id() == 0 && paths) atomicAdd(&ctr->paths, paths);
@@ -323,6 +335,7 @@ wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable s
     const bool sort = n >= P.sort_threshold;
     uint32_t counts[kWfBins];
     for (int b = 0; b < kWfBins; ++b) counts[b] = sort ? ctr->bins[b] : 0u;
+    unsigned long long paths = 0;
     for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
         uint32_t i = idx;
         if (sort) {
@@ -337,7 +350,11 @@ wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable s
         const uint32_t slot = tag & kWfSlotMask;
         const int tri = __float_as_int(h.x);
         if (tri < 0) {   // path_tracer.cpp:43-44: no hit, the path ends
+#if SOL_WF_SHADE_RESTART
+            paths += restart_slot(P, P.views, slot, P.color[slot], q);
+#else
             P.q_ended[q][append(&ctr->ended[q])] = slot;
+#endif
             continue;
         }
         const SceneView& sv = scenes.v[tag >> kWfSlotBits];
@@ -372,9 +389,15 @@ wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable s
             P.sh_d[j] = make_float4(vo.sh_dir.x, vo.sh_dir.y, vo.sh_dir.z, end ? 1.0f : 0.0f);
             P.sh_c[j] = make_float4(vo.pending.r, vo.pending.g, vo.pending.b, 0.0f);
         } else if (end) {
+#if SOL_WF_SHADE_RESTART
+            paths += restart_slot(P, P.views, slot, make_float4(ps.color.r, ps.color.g, ps.color.b, 0.0f), q);
+#else
             P.q_ended[q][append(&ctr->ended[q])] = slot;
+#endif
         }
     }
+    paths = warp_sum(paths);
+    if (lane_id() == 0 && paths) atomicAdd(&ctr->paths, paths);
 }
 
 /// K4: shadow rays; the light sample's contribution is added when unoccluded.

@@ -32,6 +32,14 @@ constexpr int kWfTraceMinBlocks = SOL_WF_TRACE_MIN_BLOCKS;
 /// Resident 256-thread blocks per SM the shading stage's registers must allow.
 constexpr int kWfShadeMinBlocks = SOL_WF_SHADE_MIN_BLOCKS;
 
+#ifndef SOL_WF_SHADE_RESTART
+#define SOL_WF_SHADE_RESTART 1
+#endif
+/// 1: a path that ends in the shade stage with no shadow ray pending (a miss,
+/// the path length, roulette, a failed BSDF sample) restarts its slot right
+/// there -- colour out, next work item, camera ray into the next extend queue
+/// -- instead of going through the ended list and the next generate stage.
+
 #ifndef SOL_WF_GEN_SMEM_VIEWS
 #define SOL_WF_GEN_SMEM_VIEWS 1
 #endif
