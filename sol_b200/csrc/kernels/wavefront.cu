@@ -350,6 +350,9 @@ wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable s
         const uint32_t slot = tag & kWfSlotMask;
         const int tri = __float_as_int(h.x);
         if (tri < 0) {   // path_tracer.cpp:43-44: no hit, the path ends
+#if SOL_WF_ORDERED_SHADOW
+            P.alt[1][i].w = -1.0f;   // no shadow ray at this extend position
+#endif
 #if SOL_WF_SHADE_RESTART
             paths += restart_slot(P, P.views, slot, P.color[slot], q);
 #else
@@ -383,12 +386,22 @@ wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable s
             P.ray_o[q][j] = make_float4(ps.org.x, ps.org.y, ps.org.z, ps.tmin);
             P.ray_d[q][j] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, d.w);
         }
+#if SOL_WF_ORDERED_SHADOW
+        // Shadow rays are staged at the extend position and compacted in
+        // extend order afterwards (wf_shadow_compact); -1 marks no ray.
+        P.alt[1][i] = make_float4(vo.sh_dir.x, vo.sh_dir.y, vo.sh_dir.z, vo.has_shadow ? (end ? 1.0f : 0.0f) : -1.0f);
+        if (vo.has_shadow) {
+            P.alt[0][i] = make_float4(vo.sh_org.x, vo.sh_org.y, vo.sh_org.z, d.w);
+            P.alt[2][i] = make_float4(vo.pending.r, vo.pending.g, vo.pending.b, 0.0f);
+        } else if (end) {
+#else
         if (vo.has_shadow) {
             const uint32_t j = append(&ctr->shadow);
             P.sh_o[j] = make_float4(vo.sh_org.x, vo.sh_org.y, vo.sh_org.z, d.w);
             P.sh_d[j] = make_float4(vo.sh_dir.x, vo.sh_dir.y, vo.sh_dir.z, end ? 1.0f : 0.0f);
             P.sh_c[j] = make_float4(vo.pending.r, vo.pending.g, vo.pending.b, 0.0f);
         } else if (end) {
+#endif
 #if SOL_WF_SHADE_RESTART
             paths += restart_slot(P, P.views, slot, make_float4(ps.color.r, ps.color.g, ps.color.b, 0.0f), q);
 #else
@@ -455,6 +468,49 @@ __device__ __forceinline__ uint32_t ray_key(const WfParams& P, float4 o, float4 
     const uint32_t octant = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
     const uint32_t key = (scene << (kWfSortBits - P.scene_bits)) | (octant << (3 * per)) | morton;
     return key & (kWfSortBins - 1u);
+}
+
+/// Ordered shadow queue (SOL_WF_ORDERED_SHADOW): the shade stage leaves each
+/// shadow ray at its extend position in the spare arrays; this kernel packs
+/// them into the shadow queue keeping their order inside each block's 1024
+/// positions (a block scan, then one atomic per block for its place), so that
+/// neighbouring lanes trace shadow rays of neighbouring pixels even when the
+/// shading ran material by material.
+__global__ void __launch_bounds__(1024) wf_shadow_compact(const WfParams* __restrict__ Pp) {
+    __shared__ uint32_t warp_counts[32];
+    __shared__ uint32_t block_base;
+    const WfParams& P = *Pp;
+    WfCounters* ctr = P.ctr;
+    const uint32_t n = ctr->extend[ctr->iter & 1u];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        float4 d = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        if (i < n) d = P.alt[1][i];
+        const bool valid = d.w >= 0.0f;
+        const unsigned ballot = __ballot_sync(0xffffffffu, valid);
+        if (lane == 0) warp_counts[warp] = __popc(ballot);
+        __syncthreads();
+        if (warp == 0) {
+            const uint32_t c = lane < (blockDim.x >> 5) ? warp_counts[lane] : 0u;
+            uint32_t incl = c;
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, off);
+                if ((int)lane >= off) incl += v;
+            }
+            warp_counts[lane] = incl - c;                     // exclusive prefix per warp
+            const uint32_t block_total = __shfl_sync(0xffffffffu, incl, 31);
+            if (lane == 0) block_base = block_total ? atomicAdd(&ctr->shadow, block_total) : 0u;
+        }
+        __syncthreads();
+        if (valid) {
+            const uint32_t at = block_base + warp_counts[warp] + __popc(ballot & ((1u << lane) - 1u));
+            P.sh_o[at] = P.alt[0][i];
+            P.sh_d[at] = d;
+            P.sh_c[at] = P.alt[2][i];
+        }
+        __syncthreads();
+    }
 }
 
 /// Reordering, step 1: the key of every queued ray and the key histogram
@@ -627,6 +683,9 @@ cudaError_t launch_wf_iteration(WfParams* params, const WfSceneTable& scenes, bo
     wf_extend<<<L.grid[1], L.block[1], trace_smem(L.block[1]), stream>>>(params, scenes);
     if (basic) wf_shade<true><<<L.grid[2], L.block[2], 0, stream>>>(params, scenes);
     else wf_shade<false><<<L.grid[2], L.block[2], 0, stream>>>(params, scenes);
+#if SOL_WF_ORDERED_SHADOW
+    wf_shadow_compact<<<4 * sms, 1024, 0, stream>>>(params);
+#endif
     if (ray_sort) launch_sort(params, 1, sms, stream);
     wf_shadow<<<L.grid[3], L.block[3], trace_smem(L.block[3]), stream>>>(params, scenes);
     wf_advance<<<1, 1, 0, stream>>>(params, handle, use_handle);

@@ -40,6 +40,12 @@ constexpr int kWfShadeMinBlocks = SOL_WF_SHADE_MIN_BLOCKS;
 /// there -- colour out, next work item, camera ray into the next extend queue
 /// -- instead of going through the ended list and the next generate stage.
 
+#ifndef SOL_WF_ORDERED_SHADOW
+#define SOL_WF_ORDERED_SHADOW 0
+#endif
+/// 1: shadow rays are packed in extend order (see wf_shadow_compact) instead
+/// of appended in shading order.
+
 #ifndef SOL_WF_GEN_SMEM_VIEWS
 #define SOL_WF_GEN_SMEM_VIEWS 1
 #endif
