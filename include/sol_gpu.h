@@ -330,13 +330,18 @@ typedef struct SolGpuBatchOptions {
 
 /* Order in which the wavefront traces each bounce's rays.  QUEUE: as the
  * stages queued them (camera rays in 8x4 pixel tiles, bounce rays in their
- * parents' order).  SORTED: counting-sorted first by scene, direction octant
- * and the Morton cell of the origin (14-bit key).  DEFAULT (0) is QUEUE, which
- * measured faster: the coarse cells lose the tiles' finer coherence.  Films
- * are the same bits either way. */
-#define SOL_GPU_RAY_ORDER_DEFAULT 0
-#define SOL_GPU_RAY_ORDER_QUEUE   1
-#define SOL_GPU_RAY_ORDER_SORTED  2
+ * parents' order, shadow rays in shading order -- material by material when
+ * hits are binned).  PACKED_SHADOWS: the same, but shadow rays packed in the
+ * order of the rays they were cast from (pixel neighbours stay neighbours
+ * when shading is binned; one packing kernel per bounce).  SORTED:
+ * counting-sorted first by scene, direction octant and the Morton cell of the
+ * origin (14-bit key).  DEFAULT (0) is QUEUE; the autotuner chooses between
+ * QUEUE and PACKED_SHADOWS (SORTED measured slower on every batch tried).
+ * Films are the same bits in every order. */
+#define SOL_GPU_RAY_ORDER_DEFAULT        0
+#define SOL_GPU_RAY_ORDER_QUEUE          1
+#define SOL_GPU_RAY_ORDER_SORTED         2
+#define SOL_GPU_RAY_ORDER_PACKED_SHADOWS 3
 
 /* Batch schedules.  WAVEFRONT: the queue-based wavefront (capacity, block size
  * and sort threshold apply).  MEGAKERNEL: one persistent megakernel launch over

@@ -21,7 +21,7 @@ ERR_UNSUPPORTED = -7
 ERR_CANCELLED = -8
 SCHEDULE_AUTO, SCHEDULE_PER_PIXEL, SCHEDULE_SPLIT = 0, 1, 2
 BATCH_WAVEFRONT, BATCH_MEGAKERNEL, BATCH_AUTO = 0, 1, 2
-RAY_ORDER_DEFAULT, RAY_ORDER_QUEUE, RAY_ORDER_SORTED = 0, 1, 2
+RAY_ORDER_DEFAULT, RAY_ORDER_QUEUE, RAY_ORDER_SORTED, RAY_ORDER_PACKED_SHADOWS = 0, 1, 2, 3
 SCENE_GPU_BVH = 1
 
 BSDF_DIFFUSE, BSDF_PHONG, BSDF_MIRROR, BSDF_GLASS, BSDF_INTERP = range(5)

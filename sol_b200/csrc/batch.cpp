@@ -42,6 +42,7 @@ struct SolGpuBatch {
     float4* d_scene_box = nullptr;    // per scene: bounds of the hierarchy's root (reordering keys)
     uint32_t* d_sort_bins = nullptr;  // reordering histogram and offsets
     bool graph_sort = false;          // the captured graph reorders the queues
+    bool graph_packed = false;        // the captured graph packs the shadow queue in extend order
     bool basic = false;               // every scene has basic shading
     unsigned long long max_iterations = 0;   // wavefront bounce-loop bound (0: the default)
     uint64_t scratch_limit = 0;       // wavefront scratch bytes per render (0: kWfScratchMaxBytes)
@@ -148,8 +149,8 @@ int build_graph(SolGpuBatch* b) {
     cudaGraph_t body = np.conditional.phGraph_out[0];
     e = cudaStreamBeginCaptureToGraph(b->capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        cudaError_t le = launch_wf_iteration(b->d_params, b->wf_table, b->basic, b->graph_sort, b->launch, handle, 1,
-                                             b->capture);
+        cudaError_t le = launch_wf_iteration(b->d_params, b->wf_table, b->basic, b->graph_sort, b->graph_packed,
+                                             b->launch, handle, 1, b->capture);
         e = cudaStreamEndCapture(b->capture, &body);
         if (e == cudaSuccess) e = le;
     }
@@ -435,11 +436,14 @@ int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVie
     if (rc != SOL_GPU_OK) return rc;
     WfParams& h = b->host;
     const bool ray_sort = b->opts.ray_order == SOL_GPU_RAY_ORDER_SORTED;
-    if (ray_sort != b->graph_sort) {
+    const bool packed = b->opts.ray_order == SOL_GPU_RAY_ORDER_PACKED_SHADOWS;
+    if (ray_sort != b->graph_sort || packed != b->graph_packed) {
         destroy_graph(b);
         b->graph_sort = ray_sort;
+        b->graph_packed = packed;
     }
     h.ray_sort = ray_sort ? 1u : 0u;
+    h.shadow_packed = packed ? 1u : 0u;
     {
         uint32_t bits = 0;
         while ((1u << bits) < b->scenes.size()) ++bits;
@@ -478,7 +482,8 @@ int render_wavefront(SolGpuBatch* b, const SolGpuConfig* config, const SolGpuVie
             // Host-driven loop: the same stages, one iteration per round trip.
             cudaGraphConditionalHandle none{};
             for (uint64_t it = 0;; ++it) {
-                e = launch_wf_iteration(b->d_params, b->wf_table, b->basic, ray_sort, b->launch, none, 0, stream);
+                e = launch_wf_iteration(b->d_params, b->wf_table, b->basic, ray_sort, packed, b->launch, none, 0,
+                                        stream);
                 if (e == cudaSuccess) e = cudaMemcpyAsync(b->h_ctr, b->d_ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
                 if (e != cudaSuccess) return cuda_fail(e, "wavefront iteration");
@@ -778,7 +783,7 @@ int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const Sol
     const uint32_t caps[] = {1u << 21, 1u << 22, 1u << 23, 1u << 24};
     const uint32_t blocks[] = {128, 256};
     const uint32_t sorts[] = {0u, 1u << 16, 0xffffffffu};
-    const int32_t orders[] = {SOL_GPU_RAY_ORDER_QUEUE, SOL_GPU_RAY_ORDER_SORTED};
+    const int32_t orders[] = {SOL_GPU_RAY_ORDER_QUEUE, SOL_GPU_RAY_ORDER_PACKED_SHADOWS};
     float best_ms = 1e30f;
     int rc = SOL_GPU_OK;
     const SolGpuBatchOptions saved = b->opts;

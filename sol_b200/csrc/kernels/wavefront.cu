@@ -20,7 +20,10 @@
 //                  next ray goes to the other parity's extend queue and the
 //                  light sample's shadow ray to the shadow queue.
 //   shadow   (K4): any-hit traversal of the shadow rays; an unoccluded light
-//                  sample adds its contribution to the path's colour.
+//                  sample adds its contribution to the path's colour.  With
+//                  the packed-shadow order, shade leaves each shadow ray at
+//                  its extend position and a packing kernel queues them in
+//                  that order first.
 //   advance      : resets the consumed queues and decides whether to loop.
 // Queue appends are warp-aggregated (one atomic per distinct target per warp).
 // The five stages form the body of a CUDA graph WHILE node whose condition the
@@ -336,6 +339,7 @@ wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable s
     uint32_t counts[kWfBins];
     for (int b = 0; b < kWfBins; ++b) counts[b] = sort ? ctr->bins[b] : 0u;
     unsigned long long paths = 0;
+    const bool packed = P.shadow_packed != 0;
     for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
         uint32_t i = idx;
         if (sort) {
@@ -350,9 +354,7 @@ wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable s
         const uint32_t slot = tag & kWfSlotMask;
         const int tri = __float_as_int(h.x);
         if (tri < 0) {   // path_tracer.cpp:43-44: no hit, the path ends
-#if SOL_WF_ORDERED_SHADOW
-            P.alt[1][i].w = -1.0f;   // no shadow ray at this extend position
-#endif
+            if (packed) P.alt[1][i].w = -1.0f;   // no shadow ray at this extend position
 #if SOL_WF_SHADE_RESTART
             paths += restart_slot(P, P.views, slot, P.color[slot], q);
 #else
@@ -386,22 +388,22 @@ wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable s
             P.ray_o[q][j] = make_float4(ps.org.x, ps.org.y, ps.org.z, ps.tmin);
             P.ray_d[q][j] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, d.w);
         }
-#if SOL_WF_ORDERED_SHADOW
-        // Shadow rays are staged at the extend position and compacted in
-        // extend order afterwards (wf_shadow_compact); -1 marks no ray.
-        P.alt[1][i] = make_float4(vo.sh_dir.x, vo.sh_dir.y, vo.sh_dir.z, vo.has_shadow ? (end ? 1.0f : 0.0f) : -1.0f);
-        if (vo.has_shadow) {
-            P.alt[0][i] = make_float4(vo.sh_org.x, vo.sh_org.y, vo.sh_org.z, d.w);
-            P.alt[2][i] = make_float4(vo.pending.r, vo.pending.g, vo.pending.b, 0.0f);
-        } else if (end) {
-#else
-        if (vo.has_shadow) {
+        if (packed) {
+            // Shadow rays are staged at the extend position and packed in
+            // extend order afterwards (wf_shadow_compact); -1 marks no ray.
+            P.alt[1][i] = make_float4(vo.sh_dir.x, vo.sh_dir.y, vo.sh_dir.z,
+                                      vo.has_shadow ? (end ? 1.0f : 0.0f) : -1.0f);
+            if (vo.has_shadow) {
+                P.alt[0][i] = make_float4(vo.sh_org.x, vo.sh_org.y, vo.sh_org.z, d.w);
+                P.alt[2][i] = make_float4(vo.pending.r, vo.pending.g, vo.pending.b, 0.0f);
+            }
+        } else if (vo.has_shadow) {
             const uint32_t j = append(&ctr->shadow);
             P.sh_o[j] = make_float4(vo.sh_org.x, vo.sh_org.y, vo.sh_org.z, d.w);
             P.sh_d[j] = make_float4(vo.sh_dir.x, vo.sh_dir.y, vo.sh_dir.z, end ? 1.0f : 0.0f);
             P.sh_c[j] = make_float4(vo.pending.r, vo.pending.g, vo.pending.b, 0.0f);
-        } else if (end) {
-#endif
+        }
+        if (!vo.has_shadow && end) {
 #if SOL_WF_SHADE_RESTART
             paths += restart_slot(P, P.views, slot, make_float4(ps.color.r, ps.color.g, ps.color.b, 0.0f), q);
 #else
@@ -470,7 +472,7 @@ __device__ __forceinline__ uint32_t ray_key(const WfParams& P, float4 o, float4 
     return key & (kWfSortBins - 1u);
 }
 
-/// Ordered shadow queue (SOL_WF_ORDERED_SHADOW): the shade stage leaves each
+/// Packed shadow queue (SOL_GPU_RAY_ORDER_PACKED_SHADOWS): the shade stage leaves each
 /// shadow ray at its extend position in the spare arrays; this kernel packs
 /// them into the shadow queue keeping their order inside each block's 1024
 /// positions (a block scan, then one atomic per block for its place), so that
@@ -675,17 +677,15 @@ cudaError_t allow_sort_smem() {
 }
 
 cudaError_t launch_wf_iteration(WfParams* params, const WfSceneTable& scenes, bool basic, bool ray_sort,
-                                const WfLaunch& L, cudaGraphConditionalHandle handle, int use_handle,
-                                cudaStream_t stream) {
+                                bool packed_shadows, const WfLaunch& L, cudaGraphConditionalHandle handle,
+                                int use_handle, cudaStream_t stream) {
     const int sms = L.sms > 0 ? L.sms : 1;
     wf_generate<<<L.grid[0], L.block[0], 0, stream>>>(params);
     if (ray_sort) launch_sort(params, 0, sms, stream);
     wf_extend<<<L.grid[1], L.block[1], trace_smem(L.block[1]), stream>>>(params, scenes);
     if (basic) wf_shade<true><<<L.grid[2], L.block[2], 0, stream>>>(params, scenes);
     else wf_shade<false><<<L.grid[2], L.block[2], 0, stream>>>(params, scenes);
-#if SOL_WF_ORDERED_SHADOW
-    wf_shadow_compact<<<4 * sms, 1024, 0, stream>>>(params);
-#endif
+    if (packed_shadows) wf_shadow_compact<<<4 * sms, 1024, 0, stream>>>(params);
     if (ray_sort) launch_sort(params, 1, sms, stream);
     wf_shadow<<<L.grid[3], L.block[3], trace_smem(L.block[3]), stream>>>(params, scenes);
     wf_advance<<<1, 1, 0, stream>>>(params, handle, use_handle);

@@ -40,12 +40,6 @@ constexpr int kWfShadeMinBlocks = SOL_WF_SHADE_MIN_BLOCKS;
 /// there -- colour out, next work item, camera ray into the next extend queue
 /// -- instead of going through the ended list and the next generate stage.
 
-#ifndef SOL_WF_ORDERED_SHADOW
-#define SOL_WF_ORDERED_SHADOW 0
-#endif
-/// 1: shadow rays are packed in extend order (see wf_shadow_compact) instead
-/// of appended in shading order.
-
 #ifndef SOL_WF_GEN_SMEM_VIEWS
 #define SOL_WF_GEN_SMEM_VIEWS 1
 #endif
@@ -145,6 +139,7 @@ struct WfParams {
     int refill_below;        // a traversal warp refills its idle lanes when fewer than this many are busy
     uint32_t keep_counts;    // 1: add this launch's paths and rays to the counters instead of restarting them
     uint32_t ray_sort;       // 1: reorder each ray queue before it is traced (see kWfSortBits)
+    uint32_t shadow_packed;  // 1: shadow rays staged at their extend position, packed in extend order
     uint32_t scene_bits;     // bits of the sort key taken by the scene index
     const float4* scene_box; // per scene: lower corner, upper corner (2 float4)
     uint32_t* sort_key;      // per queue position: the ray's key (scratch of the reordering)
@@ -182,11 +177,12 @@ cudaError_t launch_wf_init(const WfParams* params, uint32_t capacity, cudaStream
 /// `basic`: every scene has basic shading (shade's build without image
 /// textures and Interp BSDFs).
 /// `ray_sort`: reorder the extend and shadow queues before they are traced
-/// (WfParams::ray_sort must agree).  `params` is in device memory; the
+/// (WfParams::ray_sort must agree); `packed_shadows`: pack the shadow queue in
+/// extend order (WfParams::shadow_packed must agree).  `params` is in device memory; the
 /// reordering swaps queue arrays in it.
 cudaError_t launch_wf_iteration(WfParams* params, const WfSceneTable& scenes, bool basic, bool ray_sort,
-                                const WfLaunch& launch, cudaGraphConditionalHandle handle, int use_handle,
-                                cudaStream_t stream);
+                                bool packed_shadows, const WfLaunch& launch, cudaGraphConditionalHandle handle,
+                                int use_handle, cudaStream_t stream);
 /// Lets the reordering's histogram kernel use kWfSortBins * 4 bytes of shared memory (current device).
 cudaError_t allow_sort_smem();
 

@@ -52,6 +52,7 @@ def _render_both(scenes, specs, cfg, scratch_limit=0, **opts):
                                   dict(sort_threshold=0), dict(capacity=32, block_size=128),
                                   dict(ray_order=1), dict(ray_order=2, sort_threshold=0),
                                   dict(ray_order=2, host_loop=True, capacity=1000),
+                                  dict(ray_order=3, sort_threshold=0), dict(ray_order=3, capacity=777, host_loop=True),
                                   dict(host_loop=True, block_size=256), dict(schedule=1),
                                   # scratch for about two samples of every view: the samples run in chunks
                                   dict(scratch_limit=2 * 3 * 4 * 96 * 96 * 12)])
