@@ -316,6 +316,7 @@ def run_views(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=True)
         o = r.autotune(cfg, varr(r, 0))
         tune[name] = {"schedule": ["wavefront", "megakernel", "auto"][o.schedule], "capacity": o.capacity,
                       "block_size": o.block_size, "sort_threshold": o.sort_threshold,
+                      "ray_order": ["default", "queue", "sorted", "packed_shadows"][o.ray_order],
                       "seconds": time.perf_counter() - t0}
     arrays = {name: {i: varr(r, i) for i in range(warmup + steps)} for name, r in renderers.items()}
     times = {}
@@ -600,7 +601,8 @@ def run_scenes(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=True
     tune = {}
     for name, r in renderers.items():
         o = r.autotune(cfg, varr(r, 0))
-        tune[name] = {"capacity": o.capacity, "block_size": o.block_size, "sort_threshold": o.sort_threshold}
+        tune[name] = {"capacity": o.capacity, "block_size": o.block_size, "sort_threshold": o.sort_threshold,
+                      "ray_order": ["default", "queue", "sorted", "packed_shadows"][o.ray_order]}
     arrays = {name: {i: varr(r, i) for i in range(warmup + steps)} for name, r in renderers.items()}
 
     def plain(i):
