@@ -174,7 +174,7 @@ def make_workload(small: bool):
     return scene, scenes.SPHERES_CONFIG, w, h, spp
 
 
-from bench_workloads import cpu_model, cpu_renderer  # noqa: E402  (one definition for every workload)
+from bench_workloads import cpu_model, cpu_renderer, single_view_schedules  # noqa: E402  (one definition for every workload)
 
 
 def cpu_reference_mpaths(scene, cfg, w, h, target_s: float = 12.0, max_spp: int = 64):
@@ -359,6 +359,10 @@ def run_ours(args):
                       "bvh_depth": info.bvh_depth, "sah_cost": info.sah_cost,
                       "device_mb": info.device_bytes / 2**20, "build_ms": info.build_ms},
         }
+    if rank == 0 and world == 1 and not args.small and not args.no_configs:
+        # The batch schedules on this one view, for comparison with the plain launch.
+        line["batched"] = single_view_schedules(gscene, cfg, scene.camera, w, h, spp,
+                                                1000.0 * kernel_s / args.steps, 5, 3)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

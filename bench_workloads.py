@@ -110,6 +110,41 @@ def _timed(torch, flush, stream, fn, steps, warmup):
     return [a.elapsed_time(b) for a, b in ev]
 
 
+def single_view_schedules(gs, cfg, cam, w, h, spp, plain_ms: float, steps: int, warmup: int) -> dict:
+    """The batch schedules on a configuration of one view: the wavefront (16M
+    path slots, 256 threads; the capacity the views workload's autotuner
+    picks) and the multi-view megakernel, each rendering the view through
+    sol_gpu_batch_render, timed like the plain launch, with its Mpaths/s, its
+    ratio to the plain launch's and whether its film has the plain film's
+    bits."""
+    import torch
+    from sol_b200 import capi
+    from sol_b200.renderer import BatchRenderer, GpuPathTracer
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    plain = torch.zeros((3, h, w), device="cuda")
+    GpuPathTracer(gs, cfg).render_device(plain.data_ptr(), w, h, 0, spp, stream.cuda_stream)
+    paths = float(w * h * spp)
+    out = {"note": "one view through the batch entry point; the plain launch is sol_gpu_render_device",
+           "plain_mpaths_s": paths / plain_ms / 1e3}
+    for name, kw in (("wavefront", dict(capacity=1 << 24, block_size=256, schedule=capi.BATCH_WAVEFRONT)),
+                     ("multi_view_megakernel", dict(schedule=capi.BATCH_MEGAKERNEL))):
+        br = BatchRenderer([gs], **kw)
+        film = torch.zeros((3, h, w), device="cuda")
+        arr = br.views([(0, cam, w, h, 0, spp, film.data_ptr())])
+
+        def render(i, br=br, arr=arr, film=film):
+            film.zero_()
+            br.render(cfg, arr, stream.cuda_stream)
+        ms = float(np.mean(_timed(torch, flush, stream, render, steps, warmup)))
+        torch.cuda.synchronize()
+        out[name] = {"value": paths / ms / 1e3, "unit": METRIC, "ms": ms, "vs_plain": plain_ms / ms,
+                     "same_film_bits": bool(torch.equal(film, plain))}
+        br.close()
+        del film
+    return out
+
+
 def grad_check(g, fd, rel: float = GRAD_REL_TOL, floor_frac: float = 0.01) -> dict:
     """Per-parameter comparison of adjoint gradients with finite differences.
 
@@ -249,7 +284,7 @@ def run_cornell(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=Tru
     for i in range(steps):
         pt.render(img, (1 + i) * spp, spp)
     e2e_s = (time.perf_counter() - t0) / steps
-    extra = {}
+    extra = {"batched": single_view_schedules(gs, cfg, scene.camera, w, h, spp, float(np.mean(ms)), 50, 3)}
     if cpu:
         kind, run = cpu_renderer(scene, os.cpu_count() or 1)
         run(0, 1, w, h, cfg)

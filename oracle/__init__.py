@@ -84,6 +84,8 @@ def oracle_lib() -> C.CDLL:
                                           C.POINTER(C.c_float)]
         lib.oracle_debug_path.restype = C.c_uint32
         lib.oracle_pixel_seeds.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        lib.oracle_pow.argtypes = [f32p, f32p, C.c_uint32, f32p]
+        lib.oracle_pow.restype = None
         lib.oracle_pixel_seeds.restype = None
         _oracle = lib
     return _oracle
@@ -214,6 +216,16 @@ def pixel_seeds(fxy: np.ndarray) -> np.ndarray:
     fxy = np.ascontiguousarray(fxy, np.uint64)
     out = np.zeros(fxy.shape[0], np.uint32)
     oracle_lib().oracle_pixel_seeds(fxy.ctypes.data, fxy.shape[0], out.ctypes.data)
+    return out
+
+
+def pow_float(x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """The shared pow_ of core/math.h on the host, element-wise (float32)."""
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    out = np.zeros(x.shape[0], np.float32)
+    f32p = C.POINTER(C.c_float)
+    oracle_lib().oracle_pow(x.ctypes.data_as(f32p), y.ctypes.data_as(f32p), x.shape[0], out.ctypes.data_as(f32p))
     return out
 
 

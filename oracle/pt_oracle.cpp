@@ -584,6 +584,11 @@ void oracle_pcg_floats(uint64_t seed, uint32_t n, float* out) {
     for (uint32_t i = 0; i < n; ++i) out[i] = s();
 }
 
+/// The shared pow_ (core/math.h) on the host, element-wise over n pairs.
+void oracle_pow(const float* x, const float* y, uint32_t n, float* out) {
+    for (uint32_t i = 0; i < n; ++i) out[i] = pow_(x[i], y[i]);
+}
+
 /// Renderer::pixel_seed for a batch of (frame, x, y) triples.
 void oracle_pixel_seeds(const uint64_t* fxy, uint32_t n, uint32_t* out) {
     for (uint32_t i = 0; i < n; ++i) out[i] = pixel_seed(fxy[3 * i], fxy[3 * i + 1], fxy[3 * i + 2]);

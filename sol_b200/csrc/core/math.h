@@ -7,14 +7,17 @@
 // written from the mathematics and from the published methods named beside each
 // function.  The same source is compiled for the host (g++ -ffp-contract=off) and
 // for sm_100a (nvcc -fmad=false, IEEE div/sqrt), so that the CPU checker and the
-// GPU kernels produce bit-identical results: only +, -, *, /, sqrt and
-// float<->int conversions are used, all of which are correctly rounded on both
-// sides.  Transcendentals (sin/cos/pow) are evaluated by our own polynomial and
-// series code below rather than by a math library.
+// GPU kernels produce bit-identical results: only +, -, *, /, sqrt, explicit
+// double fused multiply-adds and float<->int conversions are used, all of which
+// are correctly rounded on both sides.  Transcendentals (sin/cos/pow) are
+// evaluated by our own polynomial and series code below rather than by a math
+// library.
 #pragma once
 
 #include <stdint.h>
 #include <string.h>
+
+#include "pow_tables.h"
 
 #if defined(__CUDACC__)
 #define SOL_HD __host__ __device__ __forceinline__
@@ -221,39 +224,92 @@ SOL_HD double log_pos_(double x) {
     return (double)e * 0.6931471805599453 + 2.0 * s * p;
 }
 
-/// e^z for z in [-800, 800] (clamped outside), by z = k ln2 + r with |r| <= ln2/2,
-/// e^r from its Taylor series to degree 13, and 2^k assembled from bits.
+/// Fused multiply-add a * b + c with one rounding (IEEE 754 fusedMultiplyAdd):
+/// the same bits on the host (the FMA instruction, or libm's correctly rounded
+/// fma) and on the device.
+SOL_HD double fma_(double a, double b, double c) {
+#if defined(__CUDA_ARCH__)
+    return __fma_rn(a, b, c);
+#else
+    return __builtin_fma(a, b, c);
+#endif
+}
+
+// Constant tables of pow_ (generated by gen_pow_tables.py, which states how
+// each value is computed); the device reads its copies through the read-only
+// data cache.
+#if defined(__CUDACC__)
+__device__ const double kPowInvDev[64] = SOL_POW_INV;
+__device__ const double kPowLogInvDev[64] = SOL_POW_LOG_INV;
+__device__ const double kPowExp2Dev[64] = SOL_POW_EXP2;
+#endif
+inline constexpr double kPowInvHost[64] = SOL_POW_INV;
+inline constexpr double kPowLogInvHost[64] = SOL_POW_LOG_INV;
+inline constexpr double kPowExp2Host[64] = SOL_POW_EXP2;
+#if defined(__CUDA_ARCH__)
+#define SOL_POW_TAB(name, j) __ldg(&name##Dev[j])
+#else
+#define SOL_POW_TAB(name, j) name##Host[j]
+#endif
+
+/// e^z for z in [-800, 800] (clamped outside; 0 below): z = (64 n + j) ln2/64 + r
+/// with k = 64 n + j the nearest integer to 64 z / ln 2 (found by adding
+/// 1.5 * 2^52, which leaves k in the low bits) and |r| <= ln2/128; then
+/// e^z = 2^n * 2^(j/64) * e^r, with e^r - 1 from its Taylor series to degree 6
+/// (truncation below 2^-54) and ln2/64 split in two so that k ln2/64 is exact.
 SOL_HD double exp_(double z) {
     if (z < -800.0) return 0.0;
     if (z > 800.0) z = 800.0;
-    double kf = z * 1.4426950408889634;
-    kf = kf < 0.0 ? -(double)(int64_t)(0.5 - kf) : (double)(int64_t)(kf + 0.5);
-    double r = z - kf * 0.6931471805599453;
-    double p = 1.0 / 6227020800.0;
-    p = 1.0 / 479001600.0 + r * p;
-    p = 1.0 / 39916800.0 + r * p;
-    p = 1.0 / 3628800.0 + r * p;
-    p = 1.0 / 362880.0 + r * p;
-    p = 1.0 / 40320.0 + r * p;
-    p = 1.0 / 5040.0 + r * p;
-    p = 1.0 / 720.0 + r * p;
-    p = 1.0 / 120.0 + r * p;
-    p = 1.0 / 24.0 + r * p;
-    p = 1.0 / 6.0 + r * p;
-    p = 0.5 + r * p;
-    p = 1.0 + r * p;
-    p = 1.0 + r * p;
-    int k = (int)kf;
-    // Apply 2^k in two halves so that neither factor under/overflows.
-    int k1 = k / 2, k2 = k - k1;
-    double f1 = bits_double((uint64_t)(k1 + 1023) << 52);
-    double f2 = bits_double((uint64_t)(k2 + 1023) << 52);
-    return p * f1 * f2;
+    const double shifter = 6755399441055744.0;   // 1.5 * 2^52
+    const double shifted = z * SOL_POW_INV_LN2_64 + shifter;
+    const double kd = shifted - shifter;
+    const int k = (int)(uint32_t)double_bits(shifted);
+    double r = fma_(-kd, SOL_POW_LN2_64_HI, z);
+    r = fma_(-kd, SOL_POW_LN2_64_LO, r);
+    double q = fma_(r, 1.0 / 720.0, 1.0 / 120.0);
+    q = fma_(q, r, 1.0 / 24.0);
+    q = fma_(q, r, 1.0 / 6.0);
+    q = fma_(q, r, 0.5);
+    const double em1 = fma_(q, r * r, r);
+    const double t = SOL_POW_TAB(kPowExp2, k & 63);
+    const double p = fma_(t, em1, t);
+    // 2^n in two halves so that neither factor under- or overflows.
+    const int n = k >> 6;
+    const int n1 = n / 2, n2 = n - n1;
+    return p * bits_double((uint64_t)(n1 + 1023) << 52) * bits_double((uint64_t)(n2 + 1023) << 52);
+}
+
+/// ln x for a positive, finite float, in double precision: x = 2^e m with m in
+/// [1, 2) taken from the float's bits; m times the reciprocal of the midpoint
+/// of its 64th of [1, 2) is 1 + r with |r| <= 2^-7, so ln m = ln(1 + r) -
+/// ln(that reciprocal) (tabulated), ln(1 + r) from its series to degree 7
+/// (truncation below 2^-59), and e ln2 with ln2 split in two so that e ln2 is
+/// exact in its head.
+SOL_HD double log_float_(float x) {
+    uint32_t bits = float_bits(x);
+    int e = (int)(bits >> 23) - 127;
+    if ((bits >> 23) == 0u) {   // subnormal: scale into the normal range (exact)
+        bits = float_bits(x * 8388608.0f);
+        e = (int)(bits >> 23) - 150;
+    }
+    const uint32_t mant = bits & 0x7fffffu;
+    const int j = (int)(mant >> 17);
+    const double m = bits_double(0x3ff0000000000000ull | ((uint64_t)mant << 29));
+    const double r = fma_(m, SOL_POW_TAB(kPowInv, j), -1.0);
+    double q = fma_(r, 1.0 / 7.0, -1.0 / 6.0);
+    q = fma_(q, r, 1.0 / 5.0);
+    q = fma_(q, r, -0.25);
+    q = fma_(q, r, 1.0 / 3.0);
+    q = fma_(q, r, -0.5);
+    const double l1p = fma_(q, r * r, r);
+    const double ed = (double)e;
+    return (ed * SOL_POW_LN2_HI + SOL_POW_TAB(kPowLogInv, j)) + fma_(ed, SOL_POW_LN2_LO, l1p);
 }
 
 /// x^y for x >= 0 (negative zero treated as zero), evaluated as e^(y ln x) in
-/// double precision and rounded once to float.  Special cases follow C's pow for
-/// non-negative bases: x^0 = 1, 1^y = 1, 0^y = 0 (y > 0) or +inf (y < 0).
+/// double precision (relative error near 2^-50 for |y ln x| < 100) and rounded
+/// once to float.  Special cases follow C's pow for non-negative bases: x^0 = 1,
+/// 1^y = 1, 0^y = 0 (y > 0) or +inf (y < 0).
 SOL_HD float pow_(float x, float y) {
     if (y == 0.0f || x == 1.0f) return 1.0f;
     if (x != x || y != y) return x + y;
@@ -262,8 +318,7 @@ SOL_HD float pow_(float x, float y) {
         return bits_float(0x7fc00000u);
     }
     if (float_bits(x) == 0x7f800000u) return y > 0.0f ? x : 0.0f;
-    double z = (double)y * log_pos_((double)x);
-    return (float)exp_(z);
+    return (float)exp_((double)y * log_float_(x));
 }
 
 // ---------------------------------------------------------------------------

@@ -75,6 +75,28 @@ struct SharedStackDyn {
 
 __device__ __forceinline__ Vec3 tri_vertex(float4 a) { return vec3(a.x, a.y, a.z); }
 
+__device__ __forceinline__ float fminf3(float a, float b, float c) { return fminf(fminf(a, b), c); }
+__device__ __forceinline__ float fmaxf3(float a, float b, float c) { return fmaxf(fmaxf(a, b), c); }
+
+/// Entry and (widened) exit distances of a ray against both child boxes of a
+/// node: a = c0.x and c0.y bounds, b = c1.x and c1.y bounds, c = both z bounds.
+/// (bound - org) * (1/dir) takes two correctly rounded operations per plane, so
+/// the widened exit distance stays conservative even for grazing rays (the
+/// product-with-offset form loses |org / dir| ulps to cancellation).
+__device__ __forceinline__ void child_slabs(float4 a, float4 b, float4 c, Vec3 org, Vec3 idir, float tmin,
+                                            float tmax, float& n0, float& f0, float& n1, float& f1) {
+    const float t0lx = (a.x - org.x) * idir.x, t0hx = (a.y - org.x) * idir.x;
+    const float t0ly = (a.z - org.y) * idir.y, t0hy = (a.w - org.y) * idir.y;
+    const float t0lz = (c.x - org.z) * idir.z, t0hz = (c.y - org.z) * idir.z;
+    const float t1lx = (b.x - org.x) * idir.x, t1hx = (b.y - org.x) * idir.x;
+    const float t1ly = (b.z - org.y) * idir.y, t1hy = (b.w - org.y) * idir.y;
+    const float t1lz = (c.z - org.z) * idir.z, t1hz = (c.w - org.z) * idir.z;
+    n0 = fmaxf3(fminf(t0lx, t0hx), fminf(t0ly, t0hy), fmaxf(fminf(t0lz, t0hz), tmin));
+    f0 = fminf3(fmaxf(t0lx, t0hx), fmaxf(t0ly, t0hy), fminf(fmaxf(t0lz, t0hz), tmax)) * kSlabWiden;
+    n1 = fmaxf3(fminf(t1lx, t1hx), fminf(t1ly, t1hy), fmaxf(fminf(t1lz, t1hz), tmin));
+    f1 = fminf3(fmaxf(t1lx, t1hx), fmaxf(t1ly, t1hy), fminf(fmaxf(t1lz, t1hz), tmax)) * kSlabWiden;
+}
+
 /// BVH traversal of one ray as a resumable state: start() sets it up, run()
 /// advances it.  For kAnyHit the first triangle hit inside (tmin, tmax) is
 /// kept; otherwise the closest one, with `tmax` shrunk to its distance.  `hit`
@@ -137,19 +159,8 @@ struct Traversal {
                 const float4 c = ldg4(n->b2);
                 const int4 r = __ldg(reinterpret_cast<const int4*>(n->ref));
                 if (kCount) ctr.nodes++;
-                // (bound - org) * (1/dir): two correctly rounded operations per plane, so the
-                // widened exit distance stays conservative even for grazing rays (the
-                // product-with-offset form loses |org / dir| ulps to cancellation).
-                float t0lx = (a.x - org.x) * idir.x, t0hx = (a.y - org.x) * idir.x;
-                float t0ly = (a.z - org.y) * idir.y, t0hy = (a.w - org.y) * idir.y;
-                float t0lz = (c.x - org.z) * idir.z, t0hz = (c.y - org.z) * idir.z;
-                float t1lx = (b.x - org.x) * idir.x, t1hx = (b.y - org.x) * idir.x;
-                float t1ly = (b.z - org.y) * idir.y, t1hy = (b.w - org.y) * idir.y;
-                float t1lz = (c.z - org.z) * idir.z, t1hz = (c.w - org.z) * idir.z;
-                float n0 = fmaxf(fmaxf(fminf(t0lx, t0hx), fminf(t0ly, t0hy)), fmaxf(fminf(t0lz, t0hz), tmin));
-                float f0 = fminf(fminf(fmaxf(t0lx, t0hx), fmaxf(t0ly, t0hy)), fminf(fmaxf(t0lz, t0hz), tmax)) * kSlabWiden;
-                float n1 = fmaxf(fmaxf(fminf(t1lx, t1hx), fminf(t1ly, t1hy)), fmaxf(fminf(t1lz, t1hz), tmin));
-                float f1 = fminf(fminf(fmaxf(t1lx, t1hx), fmaxf(t1ly, t1hy)), fminf(fmaxf(t1lz, t1hz), tmax)) * kSlabWiden;
+                float n0, f0, n1, f1;
+                child_slabs(a, b, c, org, idir, tmin, tmax, n0, f0, n1, f1);
                 const bool h0 = n0 <= f0, h1 = n1 <= f1;
                 if (h0 && h1) {
                     int near = r.x, far = r.y;

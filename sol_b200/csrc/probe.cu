@@ -1,13 +1,20 @@
-// Memory probes for the roofline: L2 read bandwidth of this GPU, measured on
+// Probes (bench and tests only; nothing on the rendering path uses them).
+//
+// Memory probe for the roofline: L2 read bandwidth of this GPU, measured on
 // a buffer that L2 holds (the path tracer's scene is mostly served from L2, so
 // its achieved L2 bytes per second are reported against this figure).
 //
 // The probe reads a `bytes`-long buffer `passes` times in one launch with
 // 16-byte loads that bypass L1 (ld.global.cg), one grid-stride sweep per pass,
-// after an untimed sweep that brings the buffer into L2.  Built as its own small
-// library (libsol_probe.so); nothing on the rendering path uses it.
+// after an untimed sweep that brings the buffer into L2.
+//
+// Math probe: the shared pow_ of core/math.h evaluated on the device, compiled
+// with the library's flags, so that a test can compare its bits with the host
+// build of the same source.  Built as its own small library (libsol_probe.so).
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include "core/math.h"
 
 namespace {
 
@@ -24,9 +31,25 @@ __global__ void __launch_bounds__(256) l2_read(const uint4* __restrict__ buf, si
     if (acc == 0x9e3779b9u) sink[0] = acc;   // keeps the loads; never true for a zero buffer
 }
 
+__global__ void pow_probe(const float* __restrict__ x, const float* __restrict__ y, float* __restrict__ out,
+                          uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = sol_b200::pow_(x[i], y[i]);
+}
+
 }  // namespace
 
 extern "C" {
+
+/// out[i] = pow_(x[i], y[i]) on the current device for device arrays of n
+/// floats; returns the CUDA error code of the launch (0 on success).
+int sol_probe_pow(const float* x, const float* y, float* out, uint32_t n) {
+    if (n == 0) return 0;
+    pow_probe<<<(n + 255) / 256, 256>>>(x, y, out, n);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return (int)e;
+}
 
 /// L2 read bandwidth in GB/s over a `bytes` buffer read `passes` times (best of
 /// `reps` timed launches); returns a negative value on a CUDA error.
