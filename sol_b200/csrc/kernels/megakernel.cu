@@ -205,11 +205,12 @@ pt_megakernel_lean(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index,
         while (ps.path_len < cfg.max_path_len) {
             // closest hit (path_tracer.cpp:42)
             float t = kFloatMax;
-            const int slot = traverse<false, false>(s, ps.org, ps.dir, ps.tmin, t, tc, stack);
+            float hu, hv;
+            const int slot = traverse_closest_uv<false>(s, ps.org, ps.dir, ps.tmin, t, hu, hv, tc, stack);
             ++n_rays;
             if (slot < 0) break;
             VertexOut vo;
-            shade_vertex<kBasic>(s, cfg, light_pick_prob, slot, t, ps, vo);
+            shade_vertex<kBasic>(s, cfg, light_pick_prob, slot, t, ps, vo, true, hu, hv);
             // shadow ray of this vertex (path_tracer.cpp:72-74)
             if (vo.has_shadow) {
                 float smax = 1.0f - cfg.ray_offset;

@@ -47,16 +47,19 @@ __device__ __forceinline__ void start_path(PathState& ps, const DCamera& cam, ui
 }
 
 /// Builds SoL's SurfaceInfo for a closest hit (src/triangle_mesh.cpp:78-99).
+/// With `have_uv` the hit's barycentrics are (hu, hv) from the traversal's
+/// triangle test; otherwise the test is repeated here (same inputs, same values).
 __device__ __forceinline__ Surface make_surface(const SceneView& s, int slot, Vec3 org, Vec3 dir, float t,
-                                                float tmin, int* bsdf, int* light) {
+                                                float tmin, int* bsdf, int* light, bool have_uv = false,
+                                                float hu = 0.0f, float hv = 0.0f) {
     const DTri* tp = s.tris + slot;
     const float4 p0 = ldg4(tp->v0), p1 = ldg4(tp->v1), p2 = ldg4(tp->v2);
     const Vec3 v0 = tri_vertex(p0), v1 = tri_vertex(p1), v2 = tri_vertex(p2);
     *bsdf = __float_as_int(p1.w);
     *light = __float_as_int(p2.w);
     // Barycentrics of the hit: the same test, same inputs, hence the same values.
-    float tt, u = 0.0f, v = 0.0f;
-    intersect_triangle(make_shear(org, dir), v0, v1, v2, tmin, kFloatMax, &tt, &u, &v);
+    float tt, u = hu, v = hv;
+    if (!have_uv) intersect_triangle(make_shear(org, dir), v0, v1, v2, tmin, kFloatMax, &tt, &u, &v);
     const DTriShade* sp = s.shade + slot;
     const float4 a = ldg4(sp->n0), b = ldg4(sp->n1), c = ldg4(sp->n2), d = ldg4(&sp->uv1y);
     Vec3 face_normal = triangle_normal(v0, v1, v2);
@@ -95,11 +98,12 @@ struct NoRecord {
 /// vertex (see NoRecord).
 template <class Rec, bool kBasic = false>
 __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& cfg, float light_pick_prob,
-                                             int slot, float t, PathState& ps, VertexOut& out, Rec& rec) {
+                                             int slot, float t, PathState& ps, VertexOut& out, Rec& rec,
+                                             bool have_uv = false, float hu = 0.0f, float hv = 0.0f) {
     out.end = false;
     out.has_shadow = false;
     int bsdf_id, light_id;
-    const Surface sf = make_surface(s, slot, ps.org, ps.dir, t, ps.tmin, &bsdf_id, &light_id);
+    const Surface sf = make_surface(s, slot, ps.org, ps.dir, t, ps.tmin, &bsdf_id, &light_id, have_uv, hu, hv);
     const Vec3 out_dir = -ps.dir;
     const uint32_t nl = s.num_lights;
     rec.begin(ps, sf);
@@ -131,11 +135,12 @@ __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& 
             cos_surf = cos_surf * inv_light_dist;
             in_dir = in_dir * inv_light_dist;
             const bool has_area = light.kind != SOL_GPU_LIGHT_POINT;
-            const float pdf_bounce = has_area ? bsdf_pdf<kBasic>(s, bsdf_id, in_dir, sf, out_dir) : 0.0f;
+            Rgb f;
+            float pdf_bounce;
+            bsdf_eval_pdf<kBasic>(s, bsdf_id, in_dir, sf, out_dir, has_area, &f, &pdf_bounce);
             const float pdf_light = ls.pdf_from * light_pick_prob;
             const float geom_term = ls.cos * inv_light_dist * inv_light_dist;
             const float mis = has_area ? balance_heuristic(pdf_light, pdf_bounce * geom_term) : 1.0f;
-            const Rgb f = bsdf_eval<kBasic>(s, bsdf_id, in_dir, sf, out_dir);
             const float scale = geom_term * cos_surf * mis / pdf_light;
             out.pending = ls.intensity * ps.T * f * scale;
             out.has_shadow = true;
@@ -166,9 +171,10 @@ __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& 
 /// shade_vertex for the forward render (no observer); kBasic as in shading.cuh.
 template <bool kBasic = false>
 __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& cfg, float light_pick_prob,
-                                             int slot, float t, PathState& ps, VertexOut& out) {
+                                             int slot, float t, PathState& ps, VertexOut& out, bool have_uv = false,
+                                             float hu = 0.0f, float hv = 0.0f) {
     NoRecord none;
-    shade_vertex<NoRecord, kBasic>(s, cfg, light_pick_prob, slot, t, ps, out, none);
+    shade_vertex<NoRecord, kBasic>(s, cfg, light_pick_prob, slot, t, ps, out, none, have_uv, hu, hv);
 }
 
 }  // namespace sol_b200

@@ -178,6 +178,31 @@ __device__ __forceinline__ float bsdf_pdf(const SceneView& s, int id, Vec3 in_di
     return lerp(pa, pb, tex_scalar<kBasic>(s, b.tex[0], sf.uv));
 }
 
+/// bsdf_eval and (when `want_pdf`) bsdf_pdf for the same pair of directions,
+/// as next-event estimation needs them: a Phong lobe's pow_(cos, exponent)
+/// is evaluated once for both (the same operands give the same bits, so the
+/// results are those of the two separate calls).
+template <bool kBasic = false>
+__device__ __forceinline__ void bsdf_eval_pdf(const SceneView& s, int id, Vec3 in_dir, const Surface& sf, Vec3 out_dir,
+                                              bool want_pdf, Rgb* f, float* pdf) {
+    const DBsdf b = s.bsdfs[id];
+    if (!kBasic && b.kind == SOL_GPU_BSDF_INTERP) {
+        *pdf = want_pdf ? bsdf_pdf<kBasic>(s, id, in_dir, sf, out_dir) : 0.0f;
+        *f = bsdf_eval<kBasic>(s, id, in_dir, sf, out_dir);
+        return;
+    }
+    if (b.kind == SOL_GPU_BSDF_PHONG) {
+        // bsdfs.cpp:68-70 and 87-89
+        const float ns = tex_scalar<kBasic>(s, b.tex[1], sf.uv);
+        const float p = pow_(reflect_cosine(in_dir, sf.normal(), out_dir), ns);
+        *pdf = want_pdf ? (ns + 1.0f) * p * (0.5f * kInvPi) : 0.0f;
+        *f = tex_color<kBasic>(s, b.tex[0], sf.uv) * p * (ns + 2.0f) * (0.5f * kInvPi);
+        return;
+    }
+    *pdf = want_pdf ? bsdf_pdf_basic<kBasic>(s, b, in_dir, sf, out_dir) : 0.0f;
+    *f = bsdf_eval_basic<kBasic>(s, b, in_dir, sf, out_dir);
+}
+
 struct BsdfSample {
     Vec3 in_dir;
     float pdf;

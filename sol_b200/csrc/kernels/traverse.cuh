@@ -119,6 +119,7 @@ struct Traversal {
     RayShear rs;
     float tmin, tmax;
     int node, sp, hit;
+    float hu, hv;   // barycentrics of the closest hit (kAnyHit: unused)
     uint32_t steps;
 
     template <class Stack>
@@ -131,6 +132,7 @@ struct Traversal {
         rs = make_shear(o, d);
         sp = 0;
         hit = -1;
+        hu = hv = 0.0f;
         steps = 0;
         node = active ? 0 : kStackSentinel;
         stack.put(sp++, kStackSentinel);
@@ -192,6 +194,8 @@ struct Traversal {
                     hit = (int)i;
                     tmax = t;
                     if (kAnyHit) break;
+                    hu = u;
+                    hv = w;
                 }
             }
             if (kAnyHit && hit >= 0) return true;
@@ -215,6 +219,20 @@ __device__ __forceinline__ int traverse_bounded(const DNode* __restrict__ nodes,
     tr.start(org, dir, tmin, tmax, active, stack);
     tr.run(nodes, tris, ctr, num_nodes, num_tris, max_steps, fault, stack, 0);
     tmax = tr.tmax;
+    return tr.hit;
+}
+
+/// Closest-hit traverse_bounded over a scene view that also returns the hit's
+/// barycentrics (u, v) as the triangle test computed them.
+template <bool kCount, class Stack>
+__device__ __forceinline__ int traverse_closest_uv(const SceneView& s, Vec3 org, Vec3 dir, float tmin, float& tmax,
+                                                   float& u, float& v, TraversalCounters& ctr, Stack& stack) {
+    Traversal<false, kCount, false> tr;
+    tr.start(org, dir, tmin, tmax, s.num_tris > 0, stack);
+    tr.run(s.nodes, s.tris, ctr, s.num_nodes, s.num_tris, s.max_steps, s.fault, stack, 0);
+    tmax = tr.tmax;
+    u = tr.hu;
+    v = tr.hv;
     return tr.hit;
 }
 
