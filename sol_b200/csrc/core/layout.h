@@ -5,8 +5,11 @@
 //  tris    : one 48-byte record per triangle in BVH leaf order, the three
 //            vertices for the watertight test; the w lanes carry the caller's
 //            triangle index, the BSDF and the light of the triangle.
-//  shade   : one 64-byte record per triangle in the same order: vertex normals
-//            and texture coordinates, fetched once per closest hit.
+//  shade   : one 80-byte record per triangle in the same order: vertex normals,
+//            texture coordinates, the face normal (computed from the leaf-order
+//            vertices by the shared math) and the BSDF and light of the
+//            triangle, everything a closest hit's surface needs besides the
+//            barycentrics, fetched once per closest hit.
 //  bsdfs, textures, images, lights: small tables; image texels are planar.
 #pragma once
 
@@ -40,9 +43,10 @@ struct alignas(16) DTriShade {
     float n0[3]; float uv0x;
     float n1[3]; float uv0y;
     float n2[3]; float uv1x;
-    float uv1y, uv2x, uv2y, pad;
+    float uv1y, uv2x, uv2y; int32_t bsdf;   // -1: none
+    float fn[3]; int32_t light;             // face normal normalize((v1 - v0) x (v2 - v0)); light, -1: none
 };
-static_assert(sizeof(DTriShade) == 64, "shading layout");
+static_assert(sizeof(DTriShade) == 80, "shading layout");
 
 /// Bsdf::Type (include/sol/bsdfs.h:39-43).
 enum : int32_t { kTypeDiffuse = 0, kTypeGlossy = 1, kTypeSpecular = 2 };

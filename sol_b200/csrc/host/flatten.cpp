@@ -307,7 +307,11 @@ bool flatten_scene(const SolGpuSceneDesc& d, FlatScene& out, std::string& err, b
             s.uv0x = d.tex_coords[2 * i0]; s.uv0y = d.tex_coords[2 * i0 + 1];
             s.uv1x = d.tex_coords[2 * i1]; s.uv1y = d.tex_coords[2 * i1 + 1];
             s.uv2x = d.tex_coords[2 * i2]; s.uv2y = d.tex_coords[2 * i2 + 1];
-            s.pad = 0.0f;
+            s.bsdf = t.bsdf;
+            s.light = t.light;
+            const Vec3 fn = triangle_normal(vec3(t.v0[0], t.v0[1], t.v0[2]), vec3(t.v1[0], t.v1[1], t.v1[2]),
+                                            vec3(t.v2[0], t.v2[1], t.v2[2]));
+            s.fn[0] = fn.x; s.fn[1] = fn.y; s.fn[2] = fn.z;
         }
     } else {
         DNode g{};

@@ -406,16 +406,17 @@ __device__ SOL_ADJ_OUTLINE int trace_recorded(const SceneView& s, const DConfig&
     Recorder recd;
     int K = 0;
     for (uint32_t len = 0; len < cfg.max_path_len; ++len) {
-        float t = kFloatMax;
+        float t = kFloatMax, hu, hv;
         TraversalCounters tc{0u, 0u};
-        const int slot = traverse<false, false>(s, ps.org, ps.dir, ps.tmin, t, tc);
+        LocalStack stack;
+        const int slot = traverse_closest_uv<false>(s, ps.org, ps.dir, ps.tmin, t, hu, hv, tc, stack);
         ++n_rays;
         if (slot < 0) break;
         // The host limits max_path_len to kAdjointMaxDepth; this guards the record array regardless.
         if (K >= kAdjointMaxDepth) { atomicOr(s.fault, kFaultPathLoop); break; }
         recd.R = rec + K++;
         VertexOut vo;
-        shade_vertex(s, cfg, light_pick_prob, slot, t, ps, vo, recd);
+        shade_vertex(s, cfg, light_pick_prob, slot, t, ps, vo, recd, true, hu, hv);
         if (vo.has_shadow) {
             float smax = 1.0f - cfg.ray_offset;
             const int occ = traverse<true, false>(s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc);

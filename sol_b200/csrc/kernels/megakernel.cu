@@ -127,14 +127,14 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
         if (done) break;
 
         // --- closest hit (path_tracer.cpp:42) ------------------------------
-        float t = kFloatMax;
-        const int slot = traverse<false, kCount>(s, ps.org, ps.dir, ps.tmin, t, tc, stack);
+        float t = kFloatMax, hu, hv;
+        const int slot = traverse_closest_uv<kCount>(s, ps.org, ps.dir, ps.tmin, t, hu, hv, tc, stack);
         ++n_rays;
 
         VertexOut vo;
         vo.has_shadow = false;
         vo.end = slot < 0;
-        if (!vo.end) shade_vertex<kBasic>(s, cfg, light_pick_prob, slot, t, ps, vo);
+        if (!vo.end) shade_vertex<kBasic>(s, cfg, light_pick_prob, slot, t, ps, vo, true, hu, hv);
 
         // --- shadow ray of this vertex (path_tracer.cpp:72-74) -------------
         if (vo.has_shadow) {
@@ -336,13 +336,13 @@ pt_megakernel_views(const WfView* __restrict__ views, uint32_t num_views, uint32
         }
         if (done) break;
 
-        float t = kFloatMax;
-        const int slot = traverse<false, kCount>(*s, ps.org, ps.dir, ps.tmin, t, tc, stack);
+        float t = kFloatMax, hu, hv;
+        const int slot = traverse_closest_uv<kCount>(*s, ps.org, ps.dir, ps.tmin, t, hu, hv, tc, stack);
         ++n_rays;
         VertexOut vo;
         vo.has_shadow = false;
         vo.end = slot < 0;
-        if (!vo.end) shade_vertex<kBasic>(*s, cfg, light_pick_prob, slot, t, ps, vo);
+        if (!vo.end) shade_vertex<kBasic>(*s, cfg, light_pick_prob, slot, t, ps, vo, true, hu, hv);
         if (vo.has_shadow) {
             float smax = 1.0f - cfg.ray_offset;
             const int occ = traverse<true, kCount>(*s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc, stack);

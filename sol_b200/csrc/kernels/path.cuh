@@ -46,23 +46,25 @@ __device__ __forceinline__ void start_path(PathState& ps, const DCamera& cam, ui
     ps.path_len = 0;
 }
 
-/// Builds SoL's SurfaceInfo for a closest hit (src/triangle_mesh.cpp:78-99).
-/// With `have_uv` the hit's barycentrics are (hu, hv) from the traversal's
-/// triangle test; otherwise the test is repeated here (same inputs, same values).
+/// Builds SoL's SurfaceInfo for a closest hit (src/triangle_mesh.cpp:78-99)
+/// from the triangle's shading record.  With `have_uv` the hit's barycentrics
+/// are (hu, hv) from the traversal's triangle test; otherwise the test is
+/// repeated here on the triangle's vertices (same inputs, same values).
 __device__ __forceinline__ Surface make_surface(const SceneView& s, int slot, Vec3 org, Vec3 dir, float t,
                                                 float tmin, int* bsdf, int* light, bool have_uv = false,
                                                 float hu = 0.0f, float hv = 0.0f) {
-    const DTri* tp = s.tris + slot;
-    const float4 p0 = ldg4(tp->v0), p1 = ldg4(tp->v1), p2 = ldg4(tp->v2);
-    const Vec3 v0 = tri_vertex(p0), v1 = tri_vertex(p1), v2 = tri_vertex(p2);
-    *bsdf = __float_as_int(p1.w);
-    *light = __float_as_int(p2.w);
-    // Barycentrics of the hit: the same test, same inputs, hence the same values.
-    float tt, u = hu, v = hv;
-    if (!have_uv) intersect_triangle(make_shear(org, dir), v0, v1, v2, tmin, kFloatMax, &tt, &u, &v);
     const DTriShade* sp = s.shade + slot;
-    const float4 a = ldg4(sp->n0), b = ldg4(sp->n1), c = ldg4(sp->n2), d = ldg4(&sp->uv1y);
-    Vec3 face_normal = triangle_normal(v0, v1, v2);
+    const float4 a = ldg4(sp->n0), b = ldg4(sp->n1), c = ldg4(sp->n2), d = ldg4(&sp->uv1y), e = ldg4(sp->fn);
+    *bsdf = __float_as_int(d.w);
+    *light = __float_as_int(e.w);
+    float tt, u = hu, v = hv;
+    if (!have_uv) {
+        const DTri* tp = s.tris + slot;
+        const float4 p0 = ldg4(tp->v0), p1 = ldg4(tp->v1), p2 = ldg4(tp->v2);
+        intersect_triangle(make_shear(org, dir), tri_vertex(p0), tri_vertex(p1), tri_vertex(p2), tmin, kFloatMax, &tt,
+                           &u, &v);
+    }
+    Vec3 face_normal = vec3(e.x, e.y, e.z);
     Vec3 normal = lerp3(vec3(a.x, a.y, a.z), vec3(b.x, b.y, b.z), vec3(c.x, c.y, c.z), u, v);
     Vec2 uv = lerp3(vec2(a.w, b.w), vec2(c.w, d.x), vec2(d.y, d.z), u, v);
     Surface sf;
@@ -131,7 +133,7 @@ __device__ __forceinline__ void shade_vertex(const SceneView& s, const DConfig& 
             float cos_surf = dot(in_dir, sf.normal());
             out.sh_org = sf.point;
             out.sh_dir = ls.pos - sf.point;
-            const float inv_light_dist = 1.0f / length(in_dir);
+            const float inv_light_dist = ls.inv_dist;   // 1 / length(in_dir), from the light sample
             cos_surf = cos_surf * inv_light_dist;
             in_dir = in_dir * inv_light_dist;
             const bool has_area = light.kind != SOL_GPU_LIGHT_POINT;

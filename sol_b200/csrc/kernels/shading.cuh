@@ -307,6 +307,7 @@ struct LightSample {
     Rgb intensity;
     float pdf_from;
     float cos;
+    float inv_dist;   // 1 / |pos - from|
 };
 
 __device__ __forceinline__ Vec3 ld3(const float* p) { return vec3(p[0], p[1], p[2]); }
@@ -320,6 +321,7 @@ __device__ SOL_SHADE_FN bool light_sample_area(const SceneView& s, const DLight&
         out->intensity = rgb(l.intensity[0], l.intensity[1], l.intensity[2]);
         out->pdf_from = 1.0f;
         out->cos = 1.0f;
+        out->inv_dist = 1.0f / length(out->pos - from);
         return true;
     }
     // Vec2f(sampler(), sampler()): the second coordinate is drawn first.
@@ -336,10 +338,14 @@ __device__ SOL_SHADE_FN bool light_sample_area(const SceneView& s, const DLight&
         pos = ld3(l.v0) + d * l.radius;
         n = d;
     }
-    Vec3 dir = normalize(from - pos);
+    // normalize(from - pos), keeping 1/length: |pos - from| has the same bits.
+    const Vec3 to_from = from - pos;
+    const float inv_dist = 1.0f / length(to_from);
+    Vec3 dir = to_from * inv_dist;
     float c = positive_dot(dir, n);
     if (!(c > 0.0f)) return false;
     out->pos = pos;
+    out->inv_dist = inv_dist;
     out->intensity = tex_color<kBasic>(s, l.tex, vec2(u, v));
     out->pdf_from = l.inv_area;
     out->cos = c;
