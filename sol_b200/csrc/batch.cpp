@@ -70,7 +70,7 @@ size_t pool_bytes(uint32_t c) {
     b += 9 * align256(sizeof(float4) * (size_t)c);                    // thru color ray_o[2] ray_d[2] sh_o sh_d sh_c
     b += align256(sizeof(unsigned long long) * (size_t)c);            // rng
     b += align256(sizeof(uint2) * (size_t)c);                         // item
-    b += align256(sizeof(float2) * (size_t)c);                        // hit
+    b += align256(sizeof(float4) * (size_t)c);                        // hit
     b += (2 + kWfBins) * align256(sizeof(uint32_t) * (size_t)c);      // ended queues, bins
     b += 3 * align256(sizeof(float4) * (size_t)c);                    // reordering: spare arrays
     b += align256(sizeof(uint32_t) * (size_t)c);                      // reordering: keys
@@ -106,7 +106,7 @@ int alloc_pool(SolGpuBatch* b, uint32_t capacity) {
         h.ray_d[k] = reinterpret_cast<float4*>(take(sizeof(float4) * c));
         h.q_ended[k] = reinterpret_cast<uint32_t*>(take(sizeof(uint32_t) * c));
     }
-    h.hit = reinterpret_cast<float2*>(take(sizeof(float2) * c));
+    h.hit = reinterpret_cast<float4*>(take(sizeof(float4) * c));
     h.sh_o = reinterpret_cast<float4*>(take(sizeof(float4) * c));
     h.sh_d = reinterpret_cast<float4*>(take(sizeof(float4) * c));
     h.sh_c = reinterpret_cast<float4*>(take(sizeof(float4) * c));

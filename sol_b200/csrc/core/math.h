@@ -193,37 +193,6 @@ SOL_HD void sincos_turns(float t, float* s, float* c) {
     *s = ss; *c = cc;
 }
 
-/// Natural logarithm of a positive, finite, normal or subnormal double, by
-/// splitting off the binary exponent (mantissa m in [sqrt(1/2), sqrt(2)]) and
-/// summing ln m = 2 atanh(s), s = (m - 1)/(m + 1), |s| < 0.172, to 12 terms.
-SOL_HD double log_pos_(double x) {
-    uint64_t bits = double_bits(x);
-    int e = (int)((bits >> 52) & 0x7ff);
-    if (e == 0) {                       // subnormal: scale by 2^64 first
-        x = x * 18446744073709551616.0;
-        bits = double_bits(x);
-        e = (int)((bits >> 52) & 0x7ff) - 64;
-    }
-    e -= 1023;
-    double m = bits_double((bits & 0x000fffffffffffffull) | 0x3ff0000000000000ull);
-    if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
-    double s = (m - 1.0) / (m + 1.0);
-    double s2 = s * s;
-    double p = 1.0 / 23.0;
-    p = 1.0 / 21.0 + s2 * p;
-    p = 1.0 / 19.0 + s2 * p;
-    p = 1.0 / 17.0 + s2 * p;
-    p = 1.0 / 15.0 + s2 * p;
-    p = 1.0 / 13.0 + s2 * p;
-    p = 1.0 / 11.0 + s2 * p;
-    p = 1.0 / 9.0 + s2 * p;
-    p = 1.0 / 7.0 + s2 * p;
-    p = 1.0 / 5.0 + s2 * p;
-    p = 1.0 / 3.0 + s2 * p;
-    p = 1.0 + s2 * p;
-    return (double)e * 0.6931471805599453 + 2.0 * s * p;
-}
-
 /// Fused multiply-add a * b + c with one rounding (IEEE 754 fusedMultiplyAdd):
 /// the same bits on the host (the FMA instruction, or libm's correctly rounded
 /// fma) and on the device.

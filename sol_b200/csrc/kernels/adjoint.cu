@@ -235,71 +235,62 @@ __device__ __forceinline__ void scatter_scalar_terms(const SceneView& s, const G
         }
 }
 
-/// d(eval)/d(ns) of a Phong BSDF for `in_dir`: with c the reflection cosine,
-/// eval = ks c^ns (ns + 2) / (2 pi) (bsdfs.cpp:68-70, 102-104), so
-/// d eval / d ns = ks c^ns ((ns + 2) ln c + 1) / (2 pi); zero where c = 0.
-__device__ __forceinline__ ScalarTerm exponent_term(const SceneView& s, const DBsdf& b, Vec3 in_dir, const Surface& sf,
-                                                    Vec3 out_dir, float weight) {
-    ScalarTerm t{-1, rgb(0.0f)};
-    if (b.kind != SOL_GPU_BSDF_PHONG || weight == 0.0f) return t;
-    const float c = reflect_cosine(in_dir, sf.normal(), out_dir);
-    if (!(c > 0.0f)) return t;
-    const float ns = tex_scalar(s, b.tex[1], sf.uv);
-    const float g = pow_(c, ns) * (0.5f * kInvPi) * ((ns + 2.0f) * (float)log_pos_((double)c) + 1.0f);
-    t.tex = b.tex[1];
-    t.d = tex_color(s, b.tex[0], sf.uv) * (g * weight);
-    return t;
-}
-
-/// Exponent terms of Bsdf::eval for any kind (InterpBsdf: both operands, bsdfs.cpp:185-190).
-__device__ __forceinline__ void exponent_terms(const SceneView& s, int id, Vec3 in_dir, const Surface& sf,
-                                               Vec3 out_dir, ScalarTerm* out) {
-    const DBsdf b = s.bsdfs[id];
-    out[1] = ScalarTerm{-1, rgb(0.0f)};
-    if (b.kind != SOL_GPU_BSDF_INTERP) { out[0] = exponent_term(s, b, in_dir, sf, out_dir, 1.0f); return; }
-    const float k = tex_scalar(s, b.tex[0], sf.uv);
-    out[0] = exponent_term(s, s.bsdfs[b.a], in_dir, sf, out_dir, 1.0f - k);
-    out[1] = exponent_term(s, s.bsdfs[b.b], in_dir, sf, out_dir, k);
-}
-
-/// d(eval)/d(colour value) of a non-interpolating BSDF for `in_dir`: the factor
-/// its colour texture is multiplied by (bsdfs.cpp:35-37, 102-104).
-__device__ __forceinline__ TexTerm eval_term(const SceneView& s, const DBsdf& b, Vec3 in_dir, const Surface& sf,
-                                             Vec3 out_dir) {
-    TexTerm t{-1, 0.0f};
+/// d(eval)/d(colour value) and d(eval)/d(ns) of a non-interpolating BSDF for
+/// `in_dir`, weighted by `weight` (an InterpBsdf operand's share; 1 otherwise).
+/// The colour texture's factor: kd / pi's 1 / pi (bsdfs.cpp:35-37), or with c
+/// the reflection cosine ks's c^ns (ns + 2) / (2 pi) (bsdfs.cpp:68-70,
+/// 102-104).  The Phong exponent's term: d eval / d ns = ks c^ns ((ns + 2) ln c
+/// + 1) / (2 pi), zero where c = 0.  c^ns is evaluated once for both.
+__device__ __forceinline__ void basic_terms(const SceneView& s, const DBsdf& b, Vec3 in_dir, const Surface& sf,
+                                            Vec3 out_dir, float weight, TexTerm* et, ScalarTerm* nt) {
+    *nt = ScalarTerm{-1, rgb(0.0f)};
     if (b.kind == SOL_GPU_BSDF_DIFFUSE) {
-        t.tex = b.tex[0];
-        t.scale = kInvPi;
-    } else if (b.kind == SOL_GPU_BSDF_PHONG) {
-        const float ns = tex_scalar(s, b.tex[1], sf.uv);
-        t.tex = b.tex[0];
-        t.scale = pow_(reflect_cosine(in_dir, sf.normal(), out_dir), ns) * (ns + 2.0f) * (0.5f * kInvPi);
+        *et = TexTerm{b.tex[0], kInvPi * weight};
+        return;
     }
-    return t;
+    if (b.kind != SOL_GPU_BSDF_PHONG) {
+        *et = TexTerm{-1, 0.0f};
+        return;
+    }
+    const float ns = tex_scalar(s, b.tex[1], sf.uv);
+    const float c = reflect_cosine(in_dir, sf.normal(), out_dir);
+    const float p = pow_(c, ns);
+    *et = TexTerm{b.tex[0], p * (ns + 2.0f) * (0.5f * kInvPi) * weight};
+    if (weight != 0.0f && c > 0.0f) {
+        const float g = p * (0.5f * kInvPi) * ((ns + 2.0f) * (float)log_float_(c) + 1.0f);
+        *nt = ScalarTerm{b.tex[1], tex_color(s, b.tex[0], sf.uv) * (g * weight)};
+    }
 }
 
-/// Terms of Bsdf::eval for any kind (InterpBsdf: both operands, bsdfs.cpp:185-190).
+/// basic_terms of Bsdf::eval for any kind (InterpBsdf: both operands,
+/// bsdfs.cpp:185-190): colour factors into `et`, exponent terms into `nt`.
 __device__ __forceinline__ void eval_terms(const SceneView& s, int id, Vec3 in_dir, const Surface& sf, Vec3 out_dir,
-                                           TexTerm* out) {
+                                           TexTerm* et, ScalarTerm* nt) {
     const DBsdf b = s.bsdfs[id];
-    out[1] = TexTerm{-1, 0.0f};
-    if (b.kind != SOL_GPU_BSDF_INTERP) { out[0] = eval_term(s, b, in_dir, sf, out_dir); return; }
+    et[1] = TexTerm{-1, 0.0f};
+    nt[1] = ScalarTerm{-1, rgb(0.0f)};
+    if (b.kind != SOL_GPU_BSDF_INTERP) {
+        basic_terms(s, b, in_dir, sf, out_dir, 1.0f, &et[0], &nt[0]);
+        return;
+    }
     const float k = tex_scalar(s, b.tex[0], sf.uv);
-    out[0] = eval_term(s, s.bsdfs[b.a], in_dir, sf, out_dir);
-    out[1] = eval_term(s, s.bsdfs[b.b], in_dir, sf, out_dir);
-    out[0].scale *= 1.0f - k;
-    out[1].scale *= k;
+    basic_terms(s, s.bsdfs[b.a], in_dir, sf, out_dir, 1.0f - k, &et[0], &nt[0]);
+    basic_terms(s, s.bsdfs[b.b], in_dir, sf, out_dir, k, &et[1], &nt[1]);
 }
 
-/// Terms of a basic BSDF's sampled colour (bsdfs.cpp:39-48, 72-85, 112-119, 138-165).
-__device__ __forceinline__ TexTerm sample_term(const SceneView& s, const DBsdf& b, const BsdfSample& bs,
-                                               const Surface& sf, Vec3 out_dir) {
-    if (b.kind == SOL_GPU_BSDF_MIRROR) return TexTerm{b.tex[0], 1.0f};
-    if (b.kind == SOL_GPU_BSDF_GLASS) {
-        const bool refracted = dot(bs.in_dir, sf.face_normal) < 0.0f;
-        return TexTerm{refracted ? b.tex[1] : b.tex[0], 1.0f};
+/// Terms of a basic BSDF's sampled colour (bsdfs.cpp:39-48, 72-85, 112-119,
+/// 138-165), weighted by `weight`: the specular kinds' colour texture, or
+/// basic_terms for the sampled direction.
+__device__ __forceinline__ void sample_terms(const SceneView& s, const DBsdf& b, const BsdfSample& bs,
+                                             const Surface& sf, Vec3 out_dir, float weight, TexTerm* ct,
+                                             ScalarTerm* bt) {
+    if (b.kind == SOL_GPU_BSDF_MIRROR || b.kind == SOL_GPU_BSDF_GLASS) {
+        const bool refracted = b.kind == SOL_GPU_BSDF_GLASS && dot(bs.in_dir, sf.face_normal) < 0.0f;
+        *ct = TexTerm{refracted ? b.tex[1] : b.tex[0], 1.0f * weight};
+        *bt = ScalarTerm{-1, rgb(0.0f)};
+        return;
     }
-    return eval_term(s, b, bs.in_dir, sf, out_dir);
+    basic_terms(s, b, bs.in_dir, sf, out_dir, weight, ct, bt);
 }
 
 /// Whether Light::emission returns the intensity texture (lights.cpp:94-106):
@@ -357,8 +348,7 @@ struct Recorder {
         R->s = scale;
         R->ltex = light.kind == SOL_GPU_LIGHT_POINT ? -1 : light.tex;
         R->luv = luv;
-        eval_terms(s, bsdf_id, in_dir, sf, out_dir, R->fterm);
-        exponent_terms(s, bsdf_id, in_dir, sf, out_dir, R->nterm);
+        eval_terms(s, bsdf_id, in_dir, sf, out_dir, R->fterm, R->nterm);
     }
     __device__ __forceinline__ void survival(float q, bool live) {
         R->q = q;
@@ -383,14 +373,8 @@ struct Recorder {
         R->flags |= kBounce;
         R->c = bs.color;
         R->r = r;
-        R->cterm[0] = sample_term(s, s.bsdfs[target], bs, sf, out_dir);
-        R->bterm[0] = exponent_term(s, s.bsdfs[target], bs.in_dir, sf, out_dir, other >= 0 ? k : 1.0f);
-        if (other >= 0) {
-            R->cterm[0].scale *= k;
-            R->cterm[1] = eval_term(s, s.bsdfs[other], bs.in_dir, sf, out_dir);
-            R->cterm[1].scale *= 1.0f - k;
-            R->bterm[1] = exponent_term(s, s.bsdfs[other], bs.in_dir, sf, out_dir, 1.0f - k);
-        }
+        sample_terms(s, s.bsdfs[target], bs, sf, out_dir, other >= 0 ? k : 1.0f, &R->cterm[0], &R->bterm[0]);
+        if (other >= 0) basic_terms(s, s.bsdfs[other], bs.in_dir, sf, out_dir, 1.0f - k, &R->cterm[1], &R->bterm[1]);
     }
 };
 

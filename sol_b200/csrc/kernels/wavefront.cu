@@ -310,7 +310,7 @@ wf_extend(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable 
         return scene;
     };
     auto finish = [&](uint32_t i, const Traversal<false, false, true>& tr) {
-        P.hit[i] = make_float2(__int_as_float(tr.hit), tr.tmax);
+        P.hit[i] = make_float4(__int_as_float(tr.hit), tr.tmax, tr.hu, tr.hv);
         if (sort) {
             int kind = kWfBins - 1;
             if (tr.hit >= 0) {
@@ -349,7 +349,7 @@ wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable s
             i = P.q_bins[(size_t)b * P.capacity + j];
         }
         const float4 o = P.ray_o[p][i], d = P.ray_d[p][i];
-        const float2 h = P.hit[i];
+        const float4 h = P.hit[i];
         const uint32_t tag = __float_as_uint(d.w);
         const uint32_t slot = tag & kWfSlotMask;
         const int tri = __float_as_int(h.x);
@@ -374,7 +374,7 @@ wf_shade(const WfParams* __restrict__ Pp, const __grid_constant__ WfSceneTable s
         ps.path_len = __float_as_uint(c4.w);
         ps.rng.state = P.rng[slot];
         VertexOut vo;
-        shade_vertex<kBasic>(sv, P.cfg, 1.0f / (float)sv.num_lights, tri, h.y, ps, vo);
+        shade_vertex<kBasic>(sv, P.cfg, 1.0f / (float)sv.num_lights, tri, h.y, ps, vo, true, h.z, h.w);
         bool end = vo.end;
         if (!end) {
             ++ps.path_len;

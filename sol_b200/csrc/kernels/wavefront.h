@@ -156,7 +156,7 @@ struct WfParams {
     // per queue position
     float4* ray_o[2];        // extend queue by parity: origin, tmin
     float4* ray_d[2];        //                         direction, slot | scene << kWfSlotBits (bits)
-    float2* hit;             // closest hit of extend position i: triangle slot (int bits, -1: miss), t
+    float4* hit;             // closest hit of extend position i: triangle slot (int bits, -1: miss), t, u, v
     uint32_t* q_bins;        // kWfBins * capacity extend positions
     float4* sh_o;            // shadow queue: origin, slot | scene << kWfSlotBits (bits)
     float4* sh_d;            //               direction, 1 when the path ends after it
