@@ -460,7 +460,10 @@ def run_adjoint(args, ClockSampler, load_peaks, steps=None, warmup=None, cpu=Tru
     import torch
     from sol_b200 import scenes
     from sol_b200.renderer import BatchRenderer, GpuPathTracer, GpuScene, image_l2
-    steps = steps or args.steps
+    # Each timed call takes a few milliseconds: at least 50 steps of each, so
+    # that the ratio is not one launch's jitter and the clock sampler (one
+    # sample per 100 ms) sees the timed region.
+    steps = max(steps or args.steps, 50)
     warmup = warmup or args.warmup
     W = H = 64 if args.small else 128
     SPP = 16
