@@ -18,7 +18,7 @@ namespace sol_b200 {
 #define SOL_MEGAKERNEL_MIN_BLOCKS 12  // 40 registers: the lean split kernel measured fastest here (16: 32 registers, 1.2 % slower)
 #endif
 #ifndef SOL_MEGAKERNEL_VIEWS_MIN_BLOCKS
-#define SOL_MEGAKERNEL_VIEWS_MIN_BLOCKS 16   // the multi-view megakernel: 32 registers, full occupancy
+#define SOL_MEGAKERNEL_VIEWS_MIN_BLOCKS 12   // the multi-view megakernel: 40 registers (measured faster than 16 and 10)
 #endif
 #ifndef SOL_MEGAKERNEL_SMALL_MIN_BLOCKS
 #define SOL_MEGAKERNEL_SMALL_MIN_BLOCKS 12   // 40 registers: renders of a few paths per lane, where spills cost more
