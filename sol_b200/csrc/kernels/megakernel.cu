@@ -9,12 +9,12 @@
 // exhausted.  One lane owns a pixel for all of its samples, which keeps the
 // per-pixel sum in SoL's sample order and the result bit-identical to the host.
 //
-// Small images (fewer pixels than a few per resident lane) use the split
-// schedule instead: a work item is one (pixel, sample), so the samples of a
-// pixel run on different lanes; each writes its path's colour (0 + colour, as
-// the per-pixel sum starts) to a scratch plane of its sample, and
-// sum_samples adds each pixel's colours in sample order, which is the same
-// sequence of additions as the per-pixel loop and gives the same bits.
+// Renders of more than one sample use the split schedule instead (the host's
+// AUTO choice): a work item is one (pixel, sample), so the samples of a pixel
+// run on different lanes; each writes its path's colour (0 + colour, as the
+// per-pixel sum starts) to a scratch plane of its sample, and sum_samples adds
+// each pixel's colours in sample order, which is the same sequence of
+// additions as the per-pixel loop and gives the same bits.
 //
 // One iteration of the loop traces one closest-hit ray, shades the hit (direct
 // emission with MIS, light sample + MIS, Russian roulette, BSDF sample), then
@@ -176,8 +176,11 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
 /// pt_megakernel<kCount = false, kSplit = true>, with less state live across
 /// the traversal (no per-pixel sum, sample range or loop bounds: the claim
 /// loop ends with the items and the bounce loop with the path length, and
-/// the traversal keeps its own step bound), so the 32-register build spills
-/// less.
+/// the traversal keeps its own step bound), so the register-capped builds
+/// spill less.  A warp's 32 lanes claim 32 items together (one sample of one
+/// 8x4 tile) and start them together; a lane whose path ends waits for the
+/// warp's longest path before the next claim, which measured faster than
+/// regenerating each lane's path at once (the lanes then drift apart).
 template <int kMinBlocks, bool kBasic>
 __global__ void __launch_bounds__(kMegakernelBlock, kMinBlocks)
 pt_megakernel_lean(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint32_t sample_count,
