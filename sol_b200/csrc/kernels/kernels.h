@@ -26,6 +26,14 @@ namespace sol_b200 {
 #ifndef SOL_MEGAKERNEL_SPLIT_LEAN
 #define SOL_MEGAKERNEL_SPLIT_LEAN 1   // 1: the split schedule's lean kernel (pt_megakernel_lean)
 #endif
+#ifndef SOL_LEAN_REGEN_MIN
+// The split schedule's lean kernel: idle lanes of a warp claim new work items
+// together once at least this many are idle (0: the warp claims only when all
+// 32 paths have ended).  Measured (frame / Cornell Mpaths/s): 0 -> 2455 /
+// 604, 8 -> 2593 / 654, 12 -> 2617 / 652, 16 -> 2635 / 645, 20 -> 2636 / 650,
+// 24 -> 2636 / 648, 32 -> 2419 / 589.
+#define SOL_LEAN_REGEN_MIN 20
+#endif
 #ifndef SOL_MEGAKERNEL_SHARED_STACK
 #define SOL_MEGAKERNEL_SHARED_STACK 0   // 1: first traversal-stack entries in shared memory (measured 5% slower)
 #endif

@@ -193,6 +193,74 @@ pt_megakernel_lean(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index,
     TraversalCounters tc{0u, 0u};
     uint32_t n_paths = 0, n_rays = 0, n_shadow = 0;
     LocalStack stack;
+#if SOL_LEAN_REGEN_MIN
+    // One bounce per iteration; the warp's idle lanes claim new items together
+    // once at least SOL_LEAN_REGEN_MIN of them are idle (or no lane has a
+    // path), so lanes neither wait for the warp's longest path nor drift apart
+    // one by one.  Every lane stays in the loop until the whole warp is done
+    // (the exit test is a warp-uniform vote), so the full-warp votes and the
+    // barrier see all 32 lanes; every iteration either advances a live path by
+    // one bounce or claims items, so the loop ends with the items.
+    PathState ps;
+    uint32_t k = 0, px = 0, py = 0;
+    bool alive = false, done = false;
+    while (true) {
+        __syncwarp();
+        const unsigned idle = __ballot_sync(0xffffffffu, !alive && !done);
+        const unsigned busy = __ballot_sync(0xffffffffu, alive);
+        if (busy == 0u && idle == 0u) break;
+        if (!alive && !done && (__popc(idle) >= SOL_LEAN_REGEN_MIN || busy == 0u)) {
+            const uint32_t item = claim_items(&ctr->next_item);
+            if (item >= items) {
+                done = true;
+            } else {
+                k = item / total;
+                const uint32_t it = item - k * total;
+                const uint32_t tile = it >> 5, l = it & 31u;
+                px = (tile % tiles_x) * 8u + (l & 7u);
+                py = (tile / tiles_x) * 4u + (l >> 3);
+                if (px < width && py < height) {
+                    start_path(ps, cam, sample_index + k, px, py, width, height);
+                    ++n_paths;
+                    alive = true;
+                }
+            }
+        }
+        if (alive) {
+            bool end = ps.path_len >= cfg.max_path_len;
+            if (!end) {
+                float t = kFloatMax;
+                float hu, hv;
+                const int slot = traverse_closest_uv<false>(s, ps.org, ps.dir, ps.tmin, t, hu, hv, tc, stack);
+                ++n_rays;
+                if (slot < 0) {
+                    end = true;
+                } else {
+                    VertexOut vo;
+                    shade_vertex<kBasic>(s, cfg, light_pick_prob, slot, t, ps, vo, true, hu, hv);
+                    if (vo.has_shadow) {
+                        float smax = 1.0f - cfg.ray_offset;
+                        const int occ =
+                            traverse<true, false>(s, vo.sh_org, vo.sh_dir, cfg.ray_offset, smax, tc, stack);
+                        ++n_rays;
+                        ++n_shadow;
+                        if (occ < 0) ps.color = ps.color + vo.pending;
+                    }
+                    if (vo.end) end = true;
+                    else end = ++ps.path_len >= cfg.max_path_len;
+                }
+            }
+            if (end) {
+                const Rgb c = rgb(0.0f) + ps.color;
+                float* f = scratch + (size_t)k * 3u * plane + (size_t)py * width + px;
+                f[0] = c.r;
+                f[plane] = c.g;
+                f[2 * plane] = c.b;
+                alive = false;
+            }
+        }
+    }
+#else
     while (true) {
         const uint32_t item = claim_items(&ctr->next_item);
         if (item >= items) break;
@@ -231,6 +299,7 @@ pt_megakernel_lean(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index,
         f[plane] = c.g;
         f[2 * plane] = c.b;
     }
+#endif
     __syncwarp();
     unsigned long long v0 = warp_sum_u64(n_paths), v1 = warp_sum_u64(n_rays), v2 = warp_sum_u64(n_shadow);
     if ((threadIdx.x & 31) == 0) {
