@@ -177,10 +177,11 @@ pt_megakernel(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint
 /// the traversal (no per-pixel sum, sample range or loop bounds: the claim
 /// loop ends with the items and the bounce loop with the path length, and
 /// the traversal keeps its own step bound), so the register-capped builds
-/// spill less.  A warp's 32 lanes claim 32 items together (one sample of one
-/// 8x4 tile) and start them together; a lane whose path ends waits for the
-/// warp's longest path before the next claim, which measured faster than
-/// regenerating each lane's path at once (the lanes then drift apart).
+/// spill less.  When the warp claims work is set by SOL_LEAN_REGEN_MIN: by
+/// default its idle lanes claim consecutive items together once 20 of its 32
+/// lanes are idle; with 0 the warp claims 32 items at once (one sample of one
+/// 8x4 tile) and waits for its longest path before the next claim.  Both beat
+/// regenerating each lane's path at once, which lets the lanes drift apart.
 template <int kMinBlocks, bool kBasic>
 __global__ void __launch_bounds__(kMegakernelBlock, kMinBlocks)
 pt_megakernel_lean(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index, uint32_t sample_count,
@@ -229,6 +230,7 @@ pt_megakernel_lean(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index,
         if (alive) {
             bool end = ps.path_len >= cfg.max_path_len;
             if (!end) {
+                // closest hit (path_tracer.cpp:42)
                 float t = kFloatMax;
                 float hu, hv;
                 const int slot = traverse_closest_uv<false>(s, ps.org, ps.dir, ps.tmin, t, hu, hv, tc, stack);
@@ -238,6 +240,7 @@ pt_megakernel_lean(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index,
                 } else {
                     VertexOut vo;
                     shade_vertex<kBasic>(s, cfg, light_pick_prob, slot, t, ps, vo, true, hu, hv);
+                    // shadow ray of this vertex (path_tracer.cpp:72-74)
                     if (vo.has_shadow) {
                         float smax = 1.0f - cfg.ray_offset;
                         const int occ =
@@ -251,7 +254,7 @@ pt_megakernel_lean(SceneView s, DCamera cam, DConfig cfg, uint64_t sample_index,
                 }
             }
             if (end) {
-                const Rgb c = rgb(0.0f) + ps.color;
+                const Rgb c = rgb(0.0f) + ps.color;   // path_tracer.cpp:19; the sum pass adds in sample order
                 float* f = scratch + (size_t)k * 3u * plane + (size_t)py * width + px;
                 f[0] = c.r;
                 f[plane] = c.g;
