@@ -780,7 +780,14 @@ int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const Sol
         v.sample_count = std::min<uint32_t>(v.sample_count, 4);
     }
     cudaStream_t s = b->capture;
-    const uint32_t caps[] = {1u << 21, 1u << 22, 1u << 23, 1u << 24};
+    // Pool capacities up to kMaxCapacity (64M slots, about 17 GB); those whose
+    // pool would not fit in the device's free memory (plus the pool this
+    // batch already holds) with 1 GiB to spare are skipped.
+    const uint32_t caps[] = {1u << 21, 1u << 22, 1u << 23, 1u << 24, 1u << 25, 1u << 26};
+    size_t free_bytes = 0, total_bytes = 0;
+    e = cudaMemGetInfo(&free_bytes, &total_bytes);
+    if (e != cudaSuccess) { cudaFree(scratch); return cuda_fail(e, "cudaMemGetInfo"); }
+    const size_t room = free_bytes + (b->pool ? pool_bytes(b->allocated) : 0);
     const uint32_t blocks[] = {128, 256};
     const uint32_t sorts[] = {0u, 1u << 16, 0xffffffffu};
     const int32_t orders[] = {SOL_GPU_RAY_ORDER_QUEUE, SOL_GPU_RAY_ORDER_PACKED_SHADOWS};
@@ -788,6 +795,7 @@ int sol_gpu_batch_autotune(SolGpuBatch* b, const SolGpuConfig* config, const Sol
     int rc = SOL_GPU_OK;
     const SolGpuBatchOptions saved = b->opts;
     for (uint32_t cap : caps) {
+        if (cap > kMaxCapacity || pool_bytes(cap) + (size_t(1) << 30) > room) continue;
         for (uint32_t blk : blocks) {
             for (uint32_t srt : sorts) {
                 for (int32_t order : orders) {
