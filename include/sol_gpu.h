@@ -319,7 +319,8 @@ typedef struct SolGpuView {
 
 /* Tuning of the batch renderer; zero fields take defaults. */
 typedef struct SolGpuBatchOptions {
-    uint32_t capacity;        /* path slots in flight (default: 4M, at most the work items) */
+    uint32_t capacity;        /* path slots in flight (default: 4M; at most 64M and the work items;
+                                 about 260 bytes of device memory per slot) */
     uint32_t block_size;      /* threads per block of the stages: 64, 128 or 256 (default 128) */
     uint32_t sort_threshold;  /* bin hits by BSDF kind when at least this many rays are queued
                                  (0 = always; 0xffffffff = never) */
@@ -384,8 +385,9 @@ int sol_gpu_batch_set_scratch_limit(SolGpuBatch* batch, uint64_t bytes);
  * timeout, src/render_job.cpp:42-55, bounds a host wait, not the loop). */
 int sol_gpu_batch_set_iteration_limit(SolGpuBatch* batch, uint64_t max_iterations);
 
-/* Times candidate options (capacity, block size, binning threshold, ray order; with
- * schedule AUTO also the megakernel schedule) on up to four samples per pixel of the
+/* Times candidate options (capacity 2M-64M slots, each only if its pool fits in the
+ * device's free memory with 1 GiB to spare; block size, binning threshold, ray
+ * order; with schedule AUTO also the megakernel schedule) on up to four samples per pixel of the
  * given views, rendered into scratch films, adopts the fastest and returns it
  * in `chosen`.  With `cache_path` set, a previous
  * choice for the same device and batch shape is read from that file instead,
